@@ -1,0 +1,184 @@
+/*
+ * swb200.h -- C ABI of the B200 Smith-Waterman protein DB search library
+ * (libswb200.so).  Plain pointers and sizes only; every call returns a
+ * sw_status (no exceptions, no exit()).
+ *
+ * The reference (SWhybrid) has no foreign-function layer: its GPU back end is
+ * the C++ class CUDAWorker behind the abstract Worker (src/Worker.h:82-249).
+ * These entry points are what a B200 Worker subclass calls from inside the
+ * Worker virtuals; each declaration names the reference code it replaces.
+ *
+ * Residue codes: 0..22 = "ABCDEFGHIKLMNPQRSTVWXYZ", 23 = '@', 24 = any other
+ * letter (the reference maps those to -1; both score 0 under BLOSUM62).
+ * Scores: Smith-Waterman local alignment with affine gaps, first gap residue
+ * costs gap_open + gap_extend, each further residue gap_extend, floor 0.
+ * With SW_FLAG_REFERENCE_CAP (default) a score above 65535 is reported as
+ * 65535, as the reference's 16-bit RecalcWorker pass does.
+ */
+#ifndef SWB200_H_
+#define SWB200_H_
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SWB200_ABI_VERSION 1
+
+typedef enum sw_status {
+    SW_OK = 0,
+    SW_ERR_INVALID = 1,      /* bad argument (null pointer, bad code, k out of range) */
+    SW_ERR_CUDA = 2,         /* CUDA runtime error; text in sw_last_error() */
+    SW_ERR_NOMEM = 3,        /* device or host allocation failed */
+    SW_ERR_STATE = 4,        /* call out of order (e.g. search before sw_db_load) */
+    SW_ERR_FORMAT = 5,       /* DB image: bad magic, version or checksum */
+    SW_ERR_UNSUPPORTED = 6,  /* size beyond what this build handles */
+    SW_ERR_BUSY = 7,         /* serving: admission refused, retry later */
+    SW_ERR_TIMEOUT = 8,      /* a bounded device or host wait ran out */
+    SW_ERR_NO_DEVICE = 9     /* no CUDA device / library built without GPU code */
+} sw_status;
+
+#define SW_FLAG_REFERENCE_CAP 1u   /* report min(score, 65535) like RecalcWorker */
+
+/* Search parameters.  Replaces Param (src/Param.h:59-117): matrix[32*32] is
+ * Param::plain_matrix indexed [query_code*32 + db_code], gap_open/gap_extend
+ * are Param::gapOpen/gapExtend, top_k is Param::topNum. */
+typedef struct sw_params {
+    int32_t matrix[32 * 32];
+    int32_t gap_open;
+    int32_t gap_extend;
+    int32_t top_k;          /* 1..1024 */
+    uint32_t flags;         /* SW_FLAG_* */
+} sw_params;
+
+/* One hit of a result list.  Replaces Result<int> (src/ResultList.h:8-16);
+ * index is the record's position in the DB as loaded (FASTA order), not a
+ * layout position.  Order: score descending, then index ascending. */
+typedef struct sw_hit {
+    int32_t score;
+    uint32_t reserved;
+    uint64_t index;
+} sw_hit;
+
+/* Kernel shape.  group_width threads cooperate on one pair of DB records
+ * (1 = one pair per thread, "inter-sequence"; 2..32 = warp-cooperative
+ * anti-diagonal wavefront, "intra-sequence"); rows_per_thread query rows are
+ * kept in registers per thread.  Pairs of records with more than cutover
+ * columns use the long shape, the rest the short shape. */
+typedef struct sw_kernel_config {
+    int32_t long_group_width;
+    int32_t long_rows_per_thread;
+    int32_t short_group_width;
+    int32_t short_rows_per_thread;
+    int32_t cutover;        /* columns; 0 = one shape for the whole DB */
+} sw_kernel_config;
+
+typedef struct sw_db_stats {
+    uint64_t n_records;
+    uint64_t n_residues;    /* sum of real record lengths */
+    uint64_t n_pairs;
+    uint64_t max_length;
+    uint64_t device_bytes;  /* resident DB footprint on the device */
+} sw_db_stats;
+
+typedef struct sw_run_stats {
+    double kernel_ms;       /* device time of the last call's kernels (CUDA events) */
+    double first_pass_ms;   /* device time of its first-pass kernel launches */
+    double total_ms;        /* host wall time of the last call */
+    uint64_t cells;         /* sum over queries of qlen * n_residues */
+    uint64_t rescored;      /* records re-scored by the 32-bit pass */
+    uint32_t launches;      /* kernels this library launched in the last call */
+    uint32_t queries;
+    sw_kernel_config used;  /* shape of the last plain search */
+} sw_run_stats;
+
+/* ---- parameters, encoding ------------------------------------------------ */
+
+/* BLOSUM62, open 10, extend 2, top 10, reference cap on (Param.h:59-117). */
+void sw_params_default(sw_params *p);
+
+/* Letters to residue codes.  Replaces DataPool::amino_acids_trans
+ * (src/DataPool.cpp:33-47) as used by DataPool::getQuery (:312-344) and
+ * FastaFile::nextSeq (src/FastaFile.cpp:110-145). */
+sw_status sw_encode(const char *letters, uint64_t n, uint8_t *codes);
+
+/* ---- context ------------------------------------------------------------- */
+
+/* Replaces CUDAWorker::CUDAWorker + alloc (src/CUDAWorker.cu:24-82): binds a
+ * device, copies the parameters, creates the stream. */
+sw_status sw_ctx_create(int device, const sw_params *params, struct sw_ctx **out);
+
+/* Replaces CUDAWorker::free / ~CUDAWorker. */
+sw_status sw_ctx_destroy(struct sw_ctx *ctx);
+
+/* Text of the last error on this context (never NULL). */
+const char *sw_last_error(const struct sw_ctx *ctx);
+
+/* ---- database ------------------------------------------------------------ */
+
+/* Makes a DB resident on the device.  Replaces the per-query host feed
+ * DataPool::fillChunk -> Worker::fill -> CUDAWorker::packDB -> asyncCopy
+ * (src/DataPool.cpp:171-286, src/CUDAWorker.cu:144-223): records are given
+ * once as codes back to back with n_records+1 offsets, sorted by length,
+ * paired and interleaved on the host, and uploaded. */
+sw_status sw_db_load(struct sw_ctx *ctx, const uint8_t *residues,
+                     const uint64_t *offsets, uint64_t n_records);
+
+sw_status sw_db_stats_get(const struct sw_ctx *ctx, sw_db_stats *out);
+
+/* ---- plain search: one query per call ------------------------------------ */
+
+/* Replaces CUDAWorker::setQuery + search (src/CUDAWorker.cu:84-142,224-246)
+ * plus the RecalcWorker pass (src/RecalcWorker.cpp:99-268) plus the top-k
+ * merge (src/ResultList.h:37-79, src/WorkerPool.cpp:99-105).
+ * hits: top_k entries; *n_hits receives how many have score > 0.
+ * scores: optional (NULL or n_records int32), every record's score in DB order. */
+sw_status sw_search(struct sw_ctx *ctx, const uint8_t *query, uint32_t qlen,
+                    sw_hit *hits, uint32_t *n_hits, int32_t *scores);
+
+/* Same as sw_search with the query already in device memory and no host
+ * copies; results stay on the device (d_scores: n_records int32, DB order,
+ * may be NULL).  Asynchronous: the work is only enqueued on the context's
+ * stream (call sw_sync to wait).  The device query buffer must stay valid
+ * until then.  Used to time the resident path. */
+sw_status sw_search_device(struct sw_ctx *ctx, const uint8_t *d_query,
+                           uint32_t qlen, int32_t *d_scores);
+
+/* Overrides the kernel shape chosen for plain searches (NULL = automatic). */
+sw_status sw_set_kernel_config(struct sw_ctx *ctx, const sw_kernel_config *cfg);
+
+/* Shape the library would pick for a query of this length. */
+sw_status sw_get_kernel_config(struct sw_ctx *ctx, uint32_t qlen, sw_kernel_config *cfg);
+
+sw_status sw_get_run_stats(const struct sw_ctx *ctx, sw_run_stats *out);
+
+/* Totals since the last sw_reset_totals, folded in by sw_sync.  first_pass_ms
+ * sums the device time of every first-pass kernel launch (CUDA events on the
+ * context's stream); search_ms sums whole searches. */
+typedef struct sw_totals {
+    double first_pass_ms;
+    double search_ms;
+    uint64_t first_pass_launches;
+    uint64_t launches;
+    uint64_t cells;
+    uint64_t queries;
+} sw_totals;
+
+/* Runs the context's work on a caller-owned CUDA stream (cudaStream_t passed
+ * as void*; NULL restores the context's own stream).  Replaces the two
+ * streams CUDAWorker::alloc creates (src/CUDAWorker.cu:53-82). */
+sw_status sw_set_stream(struct sw_ctx *ctx, void *cuda_stream);
+
+/* Waits for all work enqueued on the context and folds event timings into
+ * the totals. */
+sw_status sw_sync(struct sw_ctx *ctx);
+sw_status sw_reset_totals(struct sw_ctx *ctx);
+sw_status sw_get_totals(const struct sw_ctx *ctx, sw_totals *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SWB200_H_ */

@@ -1,0 +1,244 @@
+"""ctypes binding of libswb200.so (declarations in include/swb200.h).
+
+The library is built in place (``swhybrid_b200/libswb200.so``) by
+``swhybrid_b200.build``.  There is no CPU fallback: when the library or a CUDA
+device is missing, the calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libswb200.so")
+
+SW_OK = 0
+STATUS = {
+    0: "SW_OK", 1: "SW_ERR_INVALID", 2: "SW_ERR_CUDA", 3: "SW_ERR_NOMEM",
+    4: "SW_ERR_STATE", 5: "SW_ERR_FORMAT", 6: "SW_ERR_UNSUPPORTED",
+    7: "SW_ERR_BUSY", 8: "SW_ERR_TIMEOUT", 9: "SW_ERR_NO_DEVICE",
+}
+SW_FLAG_REFERENCE_CAP = 1
+
+# Every entry point include/swb200.h declares (checked by the CPU tests).
+EXPORTS = [
+    "sw_params_default", "sw_encode", "sw_ctx_create", "sw_ctx_destroy",
+    "sw_last_error", "sw_db_load", "sw_db_stats_get", "sw_search",
+    "sw_search_device", "sw_set_kernel_config", "sw_get_kernel_config",
+    "sw_get_run_stats", "sw_set_stream", "sw_sync", "sw_reset_totals", "sw_get_totals",
+]
+
+
+class SwError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+class sw_params(ctypes.Structure):
+    _fields_ = [("matrix", ctypes.c_int32 * 1024), ("gap_open", ctypes.c_int32),
+                ("gap_extend", ctypes.c_int32), ("top_k", ctypes.c_int32),
+                ("flags", ctypes.c_uint32)]
+
+
+class sw_hit(ctypes.Structure):
+    _fields_ = [("score", ctypes.c_int32), ("reserved", ctypes.c_uint32),
+                ("index", ctypes.c_uint64)]
+
+
+class sw_kernel_config(ctypes.Structure):
+    _fields_ = [("long_group_width", ctypes.c_int32), ("long_rows_per_thread", ctypes.c_int32),
+                ("short_group_width", ctypes.c_int32), ("short_rows_per_thread", ctypes.c_int32),
+                ("cutover", ctypes.c_int32)]
+
+    def as_tuple(self):
+        return (self.long_group_width, self.long_rows_per_thread, self.short_group_width,
+                self.short_rows_per_thread, self.cutover)
+
+
+class sw_db_stats(ctypes.Structure):
+    _fields_ = [("n_records", ctypes.c_uint64), ("n_residues", ctypes.c_uint64),
+                ("n_pairs", ctypes.c_uint64), ("max_length", ctypes.c_uint64),
+                ("device_bytes", ctypes.c_uint64)]
+
+
+class sw_totals(ctypes.Structure):
+    _fields_ = [("first_pass_ms", ctypes.c_double), ("search_ms", ctypes.c_double),
+                ("first_pass_launches", ctypes.c_uint64), ("launches", ctypes.c_uint64),
+                ("cells", ctypes.c_uint64), ("queries", ctypes.c_uint64)]
+
+
+class sw_run_stats(ctypes.Structure):
+    _fields_ = [("kernel_ms", ctypes.c_double), ("first_pass_ms", ctypes.c_double),
+                ("total_ms", ctypes.c_double),
+                ("cells", ctypes.c_uint64), ("rescored", ctypes.c_uint64),
+                ("launches", ctypes.c_uint32), ("queries", ctypes.c_uint32),
+                ("used", sw_kernel_config)]
+
+
+_lib = None
+
+
+def load(path: str = LIB_PATH):
+    """Load libswb200.so and declare every C-ABI signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(
+            f"{path} is missing: build it with `python -c 'import swhybrid_b200.build as b; b.build()'`")
+    L = ctypes.CDLL(path)
+    P = ctypes.c_void_p
+    u8p = ctypes.POINTER(ctypes.c_uint8)
+    L.sw_params_default.restype = None
+    L.sw_params_default.argtypes = [ctypes.POINTER(sw_params)]
+    L.sw_encode.restype = ctypes.c_int
+    L.sw_encode.argtypes = [ctypes.c_char_p, ctypes.c_uint64, u8p]
+    L.sw_ctx_create.restype = ctypes.c_int
+    L.sw_ctx_create.argtypes = [ctypes.c_int, ctypes.POINTER(sw_params), ctypes.POINTER(P)]
+    L.sw_ctx_destroy.restype = ctypes.c_int
+    L.sw_ctx_destroy.argtypes = [P]
+    L.sw_last_error.restype = ctypes.c_char_p
+    L.sw_last_error.argtypes = [P]
+    L.sw_db_load.restype = ctypes.c_int
+    L.sw_db_load.argtypes = [P, P, P, ctypes.c_uint64]
+    L.sw_db_stats_get.restype = ctypes.c_int
+    L.sw_db_stats_get.argtypes = [P, ctypes.POINTER(sw_db_stats)]
+    L.sw_search.restype = ctypes.c_int
+    L.sw_search.argtypes = [P, P, ctypes.c_uint32, ctypes.POINTER(sw_hit),
+                            ctypes.POINTER(ctypes.c_uint32), P]
+    L.sw_search_device.restype = ctypes.c_int
+    L.sw_search_device.argtypes = [P, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p]
+    L.sw_set_kernel_config.restype = ctypes.c_int
+    L.sw_set_kernel_config.argtypes = [P, ctypes.POINTER(sw_kernel_config)]
+    L.sw_get_kernel_config.restype = ctypes.c_int
+    L.sw_get_kernel_config.argtypes = [P, ctypes.c_uint32, ctypes.POINTER(sw_kernel_config)]
+    L.sw_get_run_stats.restype = ctypes.c_int
+    L.sw_get_run_stats.argtypes = [P, ctypes.POINTER(sw_run_stats)]
+    L.sw_set_stream.restype = ctypes.c_int
+    L.sw_set_stream.argtypes = [P, ctypes.c_void_p]
+    L.sw_sync.restype = ctypes.c_int
+    L.sw_sync.argtypes = [P]
+    L.sw_reset_totals.restype = ctypes.c_int
+    L.sw_reset_totals.argtypes = [P]
+    L.sw_get_totals.restype = ctypes.c_int
+    L.sw_get_totals.argtypes = [P, ctypes.POINTER(sw_totals)]
+    _lib = L
+    return L
+
+
+def default_params(gap_open=10, gap_extend=2, top_k=10, matrix=None,
+                   reference_cap=True) -> sw_params:
+    p = sw_params()
+    load().sw_params_default(ctypes.byref(p))
+    p.gap_open = gap_open
+    p.gap_extend = gap_extend
+    p.top_k = top_k
+    p.flags = SW_FLAG_REFERENCE_CAP if reference_cap else 0
+    if matrix is not None:
+        m = np.asarray(matrix, dtype=np.int32).reshape(-1)
+        for i in range(1024):
+            p.matrix[i] = int(m[i])
+    return p
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class Context:
+    """One device context with a resident DB (see include/swb200.h)."""
+
+    def __init__(self, device: int = 0, params: sw_params | None = None):
+        self.L = load()
+        self.params = params if params is not None else default_params()
+        h = ctypes.c_void_p()
+        st = self.L.sw_ctx_create(device, ctypes.byref(self.params), ctypes.byref(h))
+        if st != SW_OK:
+            raise SwError(st, "sw_ctx_create")
+        self.h = h
+        self.n_records = 0
+
+    def _check(self, st: int, what: str):
+        if st != SW_OK:
+            raise SwError(st, f"{what}: {self.L.sw_last_error(self.h).decode()}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.sw_ctx_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load_db(self, residues: np.ndarray, offsets: np.ndarray):
+        r = np.ascontiguousarray(residues, dtype=np.uint8)
+        o = np.ascontiguousarray(offsets, dtype=np.uint64)
+        self._check(self.L.sw_db_load(self.h, _ptr(r), _ptr(o), len(o) - 1), "sw_db_load")
+        self.n_records = len(o) - 1
+
+    def db_stats(self) -> sw_db_stats:
+        s = sw_db_stats()
+        self._check(self.L.sw_db_stats_get(self.h, ctypes.byref(s)), "sw_db_stats_get")
+        return s
+
+    def search(self, query: np.ndarray, want_scores: bool = False):
+        """Returns (hits as list of (score, index), scores or None)."""
+        q = np.ascontiguousarray(query, dtype=np.uint8)
+        k = self.params.top_k
+        hits = (sw_hit * k)()
+        nh = ctypes.c_uint32(0)
+        scores = np.zeros(max(self.n_records, 1), dtype=np.int32) if want_scores else None
+        self._check(self.L.sw_search(self.h, _ptr(q), len(q), hits, ctypes.byref(nh),
+                                     _ptr(scores) if want_scores else None), "sw_search")
+        out = [(hits[i].score, hits[i].index) for i in range(nh.value)]
+        return out, (scores[:self.n_records] if want_scores else None)
+
+    def search_device(self, d_query_ptr: int, qlen: int, d_scores_ptr: int | None = None):
+        self._check(self.L.sw_search_device(self.h, ctypes.c_void_p(d_query_ptr), qlen,
+                                            ctypes.c_void_p(d_scores_ptr) if d_scores_ptr else None),
+                    "sw_search_device")
+
+    def set_kernel_config(self, cfg: tuple | None):
+        if cfg is None:
+            self._check(self.L.sw_set_kernel_config(self.h, None), "sw_set_kernel_config")
+            return
+        c = sw_kernel_config(*cfg)
+        self._check(self.L.sw_set_kernel_config(self.h, ctypes.byref(c)), "sw_set_kernel_config")
+
+    def kernel_config(self, qlen: int) -> tuple:
+        c = sw_kernel_config()
+        self._check(self.L.sw_get_kernel_config(self.h, qlen, ctypes.byref(c)),
+                    "sw_get_kernel_config")
+        return c.as_tuple()
+
+    def set_stream(self, stream_handle: int | None):
+        self._check(self.L.sw_set_stream(self.h, ctypes.c_void_p(stream_handle or None)),
+                    "sw_set_stream")
+
+    def sync(self):
+        self._check(self.L.sw_sync(self.h), "sw_sync")
+
+    def reset_totals(self):
+        self._check(self.L.sw_reset_totals(self.h), "sw_reset_totals")
+
+    def totals(self) -> sw_totals:
+        t = sw_totals()
+        self._check(self.L.sw_get_totals(self.h, ctypes.byref(t)), "sw_get_totals")
+        return t
+
+    def run_stats(self) -> sw_run_stats:
+        s = sw_run_stats()
+        self._check(self.L.sw_get_run_stats(self.h, ctypes.byref(s)), "sw_get_run_stats")
+        return s

@@ -1,0 +1,130 @@
+// sw_probe.cu -- measures the packed-integer issue rates that bound the
+// Smith-Waterman first pass on the present GPU (the roofline denominator).
+//
+// Each kernel runs only register arithmetic (no memory traffic inside the
+// timed loop), at full occupancy, with several independent dependency chains
+// per thread:
+//   op 0  __viaddmax_s16x2          (fused add + max, 2 x int16)
+//   op 1  __vimax3_s16x2            (3-way max, 2 x int16)
+//   op 2  prmt.b32                  (byte permute)
+//   op 3  the first pass's per-row cell recurrence (5 DPX + 1 PRMT per row
+//         and 1 three-way max per two rows), the instruction mix of
+//         sw_wavefront.cuh without its shared-memory loads and shuffles.
+// Rates are returned in lane-operations per second (ops 0-2) and in cell
+// updates per second (op 3, two cells per row and register).
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace {
+
+__device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
+    uint32_t r;
+    asm volatile("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(sel));
+    return r;
+}
+
+template <int OP>
+__global__ void __launch_bounds__(512) rate_kernel(uint32_t* sink, int iters, uint32_t seed) {
+    uint32_t a[8];
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = (tid * 2654435761u) ^ (seed + 97u * j);
+    uint32_t b = seed | 0x00010001u, c = seed ^ 0x80008000u;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            if (OP == 0) a[j] = __viaddmax_s16x2(a[j], b, a[j ^ 1]);
+            if (OP == 1) a[j] = __vimax3_s16x2(a[j], b, a[j ^ 1]);
+            if (OP == 2) a[j] = prmt(a[j], a[j ^ 1], 0xC480u + (uint32_t)j);
+        }
+        b += c;
+    }
+    uint32_t r = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) r ^= a[j];
+    if (r == 0x9e3779b9u) sink[0] = r;
+}
+
+// 16 rows of the first-pass recurrence per iteration, profile words taken
+// from registers.
+__global__ void __launch_bounds__(512) cell_kernel(uint32_t* sink, int iters, uint32_t seed) {
+    constexpr int R = 16;
+    uint32_t H[R], E[R];
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        H[k] = (tid + k) & 0x000f000fu;
+        E[k] = 0u;
+    }
+    uint32_t S = 0, f = 0, diag = 0;
+    uint32_t A0 = seed ^ tid, A1 = seed * 3u, B0 = seed + tid, B1 = ~seed;
+    const uint32_t NOE = 0xfff4fff4u, NE = 0xfffefffeu, MIN16 = 0x80008000u;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const uint32_t wa = (k & 4) ? A1 : A0, wb = (k & 4) ? B1 : B0;
+            const uint32_t sel = (uint32_t)(k & 3) | ((uint32_t)((k & 3) | 8) << 4) |
+                                 ((uint32_t)(4 + (k & 3)) << 8) |
+                                 ((uint32_t)((4 + (k & 3)) | 8) << 12);
+            const uint32_t sc = prmt(wa, wb, sel);
+            uint32_t h = __viaddmax_s16x2_relu(diag, sc, E[k]);
+            h = __vimax_s16x2_relu(h, f);
+            diag = H[k];
+            H[k] = h;
+            const uint32_t hq = __viaddmax_s16x2(h, NOE, MIN16);
+            E[k] = __viaddmax_s16x2(E[k], NE, hq);
+            f = __viaddmax_s16x2(f, NE, hq);
+            if (k & 1) S = __vimax3_s16x2(S, H[k - 1], H[k]);
+        }
+        A0 = A0 * 1664525u + 1013904223u;
+        B0 ^= A0;
+        f = 0;
+        diag = S & 0x00ff00ffu;
+    }
+    uint32_t r = S;
+#pragma unroll
+    for (int k = 0; k < R; ++k) r ^= H[k] ^ E[k];
+    if (r == 0x9e3779b9u) sink[0] = r;
+}
+
+template <typename K>
+double time_kernel(K kern, int sms, int iters, uint32_t* sink, double work_per_thread) {
+    const int blocks = sms * 4, threads = 512;
+    kern<<<blocks, threads>>>(sink, iters / 8, 12345u);  // warm-up
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+    kern<<<blocks, threads>>>(sink, iters, 777u);
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (cudaGetLastError() != cudaSuccess || ms <= 0.f) return -1.0;
+    return (double)blocks * threads * work_per_thread * iters / (ms * 1e-3);
+}
+
+}  // namespace
+
+// out[0..3] = rates of ops 0..3 (see the file comment); out[4] = SM count;
+// out[5] = SM clock in MHz reported by the device attribute.  Returns 0 on
+// success.
+extern "C" int swprobe_rates(int device, double* out, int iters) {
+    if (cudaSetDevice(device) != cudaSuccess) return 1;
+    int sms = 0, clk = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaDeviceGetAttribute(&clk, cudaDevAttrClockRate, device);
+    uint32_t* sink = nullptr;
+    if (cudaMalloc(&sink, 64) != cudaSuccess) return 2;
+    if (iters <= 0) iters = 4096;
+    out[0] = time_kernel(rate_kernel<0>, sms, iters, sink, 8.0 * 2);
+    out[1] = time_kernel(rate_kernel<1>, sms, iters, sink, 8.0 * 2);
+    out[2] = time_kernel(rate_kernel<2>, sms, iters, sink, 8.0);
+    out[3] = time_kernel(cell_kernel, sms, iters / 4, sink, 16.0 * 2);
+    out[4] = sms;
+    out[5] = clk / 1000.0;
+    cudaFree(sink);
+    return cudaGetLastError() == cudaSuccess ? 0 : 3;
+}

@@ -1,0 +1,762 @@
+// sw_engine.cu -- host side of libswb200: context, resident DB layout, kernel
+// shape selection and the plain search sequence behind the C ABI (swb200.h).
+//
+// Reference flow this replaces (SWhybrid, CUDA build): per query and per
+// 256 MB chunk, DataPool::fillChunk reads batches from disk, CUDAWorker::packDB
+// re-packs them on the host, asyncCopy ships the whole chunk over PCIe,
+// kernelLaunch runs, and a synchronous cudaMemcpy brings the scores back
+// (src/Worker.cpp:175-200, src/CUDAWorker.cu:144-246); overflowed records are
+// re-scored on the host afterwards (src/RecalcWorker.cpp:99-268) and top-k is
+// merged by list insertion (src/ResultList.h:37-79).
+//
+// Here the DB is laid out once (sorted by length, paired, column-interleaved)
+// and stays in HBM; a search is: query H2D (a few KB), first-pass kernel(s),
+// 32-bit re-score of the flagged records, device top-k, D2H of k hits.
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/swb200.h"
+#include "sw_aux.h"
+#include "sw_device.cuh"
+#include "sw_engine.h"
+#include "sw_registry.h"
+
+namespace swb {
+extern const WfKernel wf_table_t1[];
+extern const int wf_table_t1_n;
+extern const WfKernel wf_table_t2[];
+extern const int wf_table_t2_n;
+extern const WfKernel wf_table_t4[];
+extern const int wf_table_t4_n;
+extern const WfKernel wf_table_t8[];
+extern const int wf_table_t8_n;
+extern const WfKernel wf_table_t16[];
+extern const int wf_table_t16_n;
+extern const WfKernel wf_table_t32[];
+extern const int wf_table_t32_n;
+
+const WfKernel* wf_kernels(int* n) {
+    static std::vector<WfKernel> all;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        auto add = [](const WfKernel* t, int m) { all.insert(all.end(), t, t + m); };
+        add(wf_table_t1, wf_table_t1_n);
+        add(wf_table_t2, wf_table_t2_n);
+        add(wf_table_t4, wf_table_t4_n);
+        add(wf_table_t8, wf_table_t8_n);
+        add(wf_table_t16, wf_table_t16_n);
+        add(wf_table_t32, wf_table_t32_n);
+    });
+    *n = (int)all.size();
+    return all.data();
+}
+
+const WfKernel* find_kernel(int T, int R) {
+    int n = 0;
+    const WfKernel* k = wf_kernels(&n);
+    for (int i = 0; i < n; ++i)
+        if (k[i].T == T && k[i].R == R) return &k[i];
+    return nullptr;
+}
+
+}  // namespace swb
+
+using namespace swb;
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+
+#define SW_SET(ctx, code, ...)                                              \
+    do {                                                                    \
+        char _b[512];                                                       \
+        snprintf(_b, sizeof(_b), __VA_ARGS__);                              \
+        if (ctx) (ctx)->err = _b;                                           \
+        return code;                                                        \
+    } while (0)
+
+#define SW_CUDA(ctx, call)                                                  \
+    do {                                                                    \
+        cudaError_t _e = (call);                                            \
+        if (_e != cudaSuccess)                                              \
+            SW_SET(ctx, SW_ERR_CUDA, "%s failed: %s (%s:%d)", #call,        \
+                   cudaGetErrorString(_e), __FILE__, __LINE__);             \
+    } while (0)
+
+namespace {
+
+template <typename T>
+cudaError_t dev_alloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    return cudaMalloc((void**)p, count * sizeof(T));
+}
+
+template <typename T>
+void dev_free(T*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// parameters and encoding
+// ---------------------------------------------------------------------------
+
+// BLOSUM62 in the reference's code order (A B C D E F G H I K L M N P Q R S T
+// V W X Y Z), the table of src/Param.h:8-51.  Rows/columns 23..31 are zero.
+static const int8_t kBlosum62[23][23] = {
+    {4, -2, 0, -2, -1, -2, 0, -2, -1, -1, -1, -1, -2, -1, -1, -1, 1, 0, 0, -3, 0, -2, -1},
+    {-2, 4, -3, 4, 1, -3, -1, 0, -3, 0, -4, -3, 3, -2, 0, -1, 0, -1, -3, -4, -1, -3, 1},
+    {0, -3, 9, -3, -4, -2, -3, -3, -1, -3, -1, -1, -3, -3, -3, -3, -1, -1, -1, -2, -2, -2, -3},
+    {-2, 4, -3, 6, 2, -3, -1, -1, -3, -1, -4, -3, 1, -1, 0, -2, 0, -1, -3, -4, -1, -3, 1},
+    {-1, 1, -4, 2, 5, -3, -2, 0, -3, 1, -3, -2, 0, -1, 2, 0, 0, -1, -2, -3, -1, -2, 4},
+    {-2, -3, -2, -3, -3, 6, -3, -1, 0, -3, 0, 0, -3, -4, -3, -3, -2, -2, -1, 1, -1, 3, -3},
+    {0, -1, -3, -1, -2, -3, 6, -2, -4, -2, -4, -3, 0, -2, -2, -2, 0, -2, -3, -2, -1, -3, -2},
+    {-2, 0, -3, -1, 0, -1, -2, 8, -3, -1, -3, -2, 1, -2, 0, 0, -1, -2, -3, -2, -1, 2, 0},
+    {-1, -3, -1, -3, -3, 0, -4, -3, 4, -3, 2, 1, -3, -3, -3, -3, -2, -1, 3, -3, -1, -1, -3},
+    {-1, 0, -3, -1, 1, -3, -2, -1, -3, 5, -2, -1, 0, -1, 1, 2, 0, -1, -2, -3, -1, -2, 1},
+    {-1, -4, -1, -4, -3, 0, -4, -3, 2, -2, 4, 2, -3, -3, -2, -2, -2, -1, 1, -2, -1, -1, -3},
+    {-1, -3, -1, -3, -2, 0, -3, -2, 1, -1, 2, 5, -2, -2, 0, -1, -1, -1, 1, -1, -1, -1, -1},
+    {-2, 3, -3, 1, 0, -3, 0, 1, -3, 0, -3, -2, 6, -2, 0, 0, 1, 0, -3, -4, -1, -2, 0},
+    {-1, -2, -3, -1, -1, -4, -2, -2, -3, -1, -3, -2, -2, 7, -1, -2, -1, -1, -2, -4, -2, -3, -1},
+    {-1, 0, -3, 0, 2, -3, -2, 0, -3, 1, -2, 0, 0, -1, 5, 1, 0, -1, -2, -2, -1, -1, 3},
+    {-1, -1, -3, -2, 0, -3, -2, 0, -3, 2, -2, -1, 0, -2, 1, 5, -1, -1, -3, -3, -1, -2, 0},
+    {1, 0, -1, 0, 0, -2, 0, -1, -2, 0, -2, -1, 1, -1, 0, -1, 4, 1, -2, -3, 0, -2, 0},
+    {0, -1, -1, -1, -1, -2, -2, -2, -1, -1, -1, -1, 0, -1, -1, -1, 1, 5, 0, -2, 0, -2, -1},
+    {0, -3, -1, -3, -2, -1, -3, -3, 3, -2, 1, 1, -3, -2, -2, -3, -2, 0, 4, -3, -1, -1, -2},
+    {-3, -4, -2, -4, -3, 1, -2, -2, -3, -3, -2, -1, -4, -4, -2, -3, -3, -2, -3, 11, -2, 2, -3},
+    {0, -1, -2, -1, -1, -1, -1, -1, -1, -1, -1, -1, -1, -2, -1, -1, 0, 0, -1, -2, -1, -1, -1},
+    {-2, -3, -2, -3, -2, 3, -3, 2, -1, -2, -1, -1, -2, -3, -1, -2, -2, -2, -1, 2, -1, 7, -2},
+    {-1, 1, -3, 1, 4, -3, -2, 0, -3, 1, -3, -1, 0, -1, 3, 0, 0, -1, -2, -3, -1, -2, 4},
+};
+
+extern "C" void sw_params_default(sw_params* p) {
+    if (!p) return;
+    memset(p, 0, sizeof(*p));
+    for (int i = 0; i < 23; ++i)
+        for (int j = 0; j < 23; ++j) p->matrix[i * 32 + j] = kBlosum62[i][j];
+    p->gap_open = 10;
+    p->gap_extend = 2;
+    p->top_k = 10;
+    p->flags = SW_FLAG_REFERENCE_CAP;
+}
+
+extern "C" sw_status sw_encode(const char* letters, uint64_t n, uint8_t* codes) {
+    if ((!letters || !codes) && n) return SW_ERR_INVALID;
+    static const char* alpha = "ABCDEFGHIKLMNPQRSTVWXYZ";
+    uint8_t tab[256];
+    memset(tab, kZeroCode, sizeof(tab));
+    for (int i = 0; alpha[i]; ++i) {
+        tab[(uint8_t)alpha[i]] = (uint8_t)i;
+        tab[(uint8_t)(alpha[i] - 'A' + 'a')] = (uint8_t)i;
+    }
+    tab[(uint8_t)'@'] = 23;
+    for (uint64_t i = 0; i < n; ++i) codes[i] = tab[(uint8_t)letters[i]];
+    return SW_OK;
+}
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+
+extern "C" const char* sw_last_error(const sw_ctx* ctx) {
+    return ctx ? ctx->err.c_str() : "null context";
+}
+
+static sw_status validate_params(sw_ctx* ctx, const sw_params* p) {
+    if (p->gap_open < 0 || p->gap_extend < 0 || p->gap_open + p->gap_extend > 1000)
+        SW_SET(ctx, SW_ERR_INVALID, "gap costs out of range (open %d, extend %d)", p->gap_open,
+               p->gap_extend);
+    if (p->top_k < 1 || p->top_k > kMaxTopK)
+        SW_SET(ctx, SW_ERR_INVALID, "top_k %d outside 1..%d", p->top_k, kMaxTopK);
+    for (int i = 0; i < 1024; ++i)
+        if (p->matrix[i] < -127 || p->matrix[i] > 127)
+            SW_SET(ctx, SW_ERR_INVALID, "matrix entry %d = %d outside -127..127", i,
+                   p->matrix[i]);
+    return SW_OK;
+}
+
+extern "C" sw_status sw_ctx_create(int device, const sw_params* params, sw_ctx** out) {
+    if (!out) return SW_ERR_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return SW_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) return SW_ERR_INVALID;
+    sw_ctx* ctx = new sw_ctx();
+    ctx->device = device;
+    if (params) ctx->params = *params;
+    else sw_params_default(&ctx->params);
+    sw_status st = validate_params(ctx, &ctx->params);
+    if (st != SW_OK) {
+        delete ctx;
+        return st;
+    }
+    auto fail = [&](sw_status s) {
+        sw_ctx_destroy(ctx);
+        return s;
+    };
+    if (cudaSetDevice(device) != cudaSuccess) return fail(SW_ERR_CUDA);
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return fail(SW_ERR_CUDA);
+    ctx->num_sms = prop.multiProcessorCount;
+    ctx->max_smem = (int)prop.sharedMemPerBlockOptin;
+    if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(SW_ERR_CUDA);
+    ctx->stream = ctx->own_stream;
+    for (auto& e : ctx->ev)
+        if (cudaEventCreate(&e) != cudaSuccess) return fail(SW_ERR_CUDA);
+    // matrix: int8 copy; codes >= 24 (zero code, pads) score 0
+    int8_t mat8[1024];
+    int hi = 0;
+    for (int i = 0; i < 32; ++i)
+        for (int j = 0; j < 32; ++j) {
+            int v = (i >= kZeroCode || j >= kZeroCode) ? 0 : ctx->params.matrix[i * 32 + j];
+            mat8[i * 32 + j] = (int8_t)v;
+            hi = std::max(hi, v);
+        }
+    ctx->max_score = hi;
+    if (dev_alloc(&ctx->d_mat, 1024) != cudaSuccess) return fail(SW_ERR_NOMEM);
+    if (cudaMemcpy(ctx->d_mat, mat8, 1024, cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(SW_ERR_CUDA);
+    if (dev_alloc(&ctx->d_counters, 16) != cudaSuccess) return fail(SW_ERR_NOMEM);
+    // every first-pass shape may use the opt-in shared-memory maximum
+    int nk = 0;
+    const WfKernel* ks = wf_kernels(&nk);
+    for (int i = 0; i < nk; ++i)
+        if (cudaFuncSetAttribute(ks[i].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 ctx->max_smem) != cudaSuccess)
+            return fail(SW_ERR_CUDA);
+    *out = ctx;
+    return SW_OK;
+}
+
+static void free_db(sw_ctx* ctx) {
+    dev_free(ctx->d_db);
+    dev_free(ctx->d_pairs);
+    dev_free(ctx->d_perm);
+    dev_free(ctx->d_bnd);
+    dev_free(ctx->d_scores);
+    dev_free(ctx->d_scores_rec);
+    dev_free(ctx->d_ovf);
+    dev_free(ctx->d_keys[0]);
+    dev_free(ctx->d_keys[1]);
+    ctx->n_records = 0;
+    ctx->n_pairs = 0;
+    ctx->pair_ncols.clear();
+    ctx->db_loaded = false;
+}
+
+extern "C" sw_status sw_ctx_destroy(sw_ctx* ctx) {
+    if (!ctx) return SW_ERR_INVALID;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
+    free_db(ctx);
+    dev_free(ctx->d_mat);
+    dev_free(ctx->d_counters);
+    dev_free(ctx->d_query);
+    if (ctx->h_query) cudaFreeHost(ctx->h_query);
+    if (ctx->h_keys) cudaFreeHost(ctx->h_keys);
+    for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    for (auto* v : {&ctx->pending, &ctx->spare})
+        for (auto& m : *v)
+            for (auto& e : m.e) cudaEventDestroy(e);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return SW_OK;
+}
+
+// ---------------------------------------------------------------------------
+// database layout
+// ---------------------------------------------------------------------------
+
+extern "C" sw_status sw_db_load(sw_ctx* ctx, const uint8_t* residues, const uint64_t* offsets,
+                                uint64_t n) {
+    if (!ctx) return SW_ERR_INVALID;
+    if (!offsets || (n && !residues && offsets[n] != offsets[0]))
+        SW_SET(ctx, SW_ERR_INVALID, "null residues/offsets");
+    if (n >= (1ull << 31)) SW_SET(ctx, SW_ERR_UNSUPPORTED, "too many records (%llu)",
+                                  (unsigned long long)n);
+    SW_CUDA(ctx, cudaSetDevice(ctx->device));
+    SW_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    free_db(ctx);
+    std::vector<uint32_t> len(n);
+    uint64_t total = 0, maxlen = 0;
+    for (uint64_t i = 0; i < n; ++i) {
+        if (offsets[i + 1] < offsets[i]) SW_SET(ctx, SW_ERR_INVALID, "offsets not monotone at %llu",
+                                                (unsigned long long)i);
+        const uint64_t l = offsets[i + 1] - offsets[i];
+        if (l >= (1ull << 30)) SW_SET(ctx, SW_ERR_UNSUPPORTED, "record %llu too long",
+                                      (unsigned long long)i);
+        len[i] = (uint32_t)l;
+        total += l;
+        maxlen = std::max<uint64_t>(maxlen, l);
+    }
+    const uint8_t* base = residues ? residues + offsets[0] : nullptr;
+    for (uint64_t i = 0; i < total; ++i)
+        if (base[i] > 24) SW_SET(ctx, SW_ERR_INVALID, "residue code %d at %llu (codes are 0..24)",
+                                 base[i], (unsigned long long)i);
+    // sort by length (longest first), stable in record order
+    std::vector<uint32_t> order(n);
+    std::iota(order.begin(), order.end(), 0u);
+    std::stable_sort(order.begin(), order.end(),
+                     [&](uint32_t a, uint32_t b) { return len[a] > len[b]; });
+    const uint64_t npairs_all = (n + 1) / 2;
+    std::vector<Pair2> pairs(npairs_all);
+    uint64_t units = 0, nonempty = 0;
+    for (uint64_t p = 0; p < npairs_all; ++p) {
+        const uint32_t nc = len[order[2 * p]];
+        pairs[p].off16 = (uint32_t)units;
+        pairs[p].ncols = nc;
+        units += (nc + 7) / 8;
+        if (nc > 0) nonempty = p + 1;
+        if (units >= (1ull << 32)) SW_SET(ctx, SW_ERR_UNSUPPORTED, "DB too large for 32-bit unit offsets");
+    }
+    std::vector<uint8_t> stream((size_t)units * 16, (uint8_t)kZeroCode);
+    for (uint64_t p = 0; p < npairs_all; ++p) {
+        uint8_t* dst = stream.data() + (size_t)pairs[p].off16 * 16;
+        for (int lane = 0; lane < 2; ++lane) {
+            const uint64_t k = 2 * p + lane;
+            if (k >= n) break;
+            const uint32_t r = order[k];
+            const uint8_t* src = base + (offsets[r] - offsets[0]);
+            for (uint32_t c = 0; c < len[r]; ++c) dst[2 * (size_t)c + lane] = src[c];
+        }
+    }
+    std::vector<uint32_t> perm(n);
+    for (uint64_t k = 0; k < n; ++k) perm[k] = order[k];
+
+    ctx->n_records = (int64_t)n;
+    ctx->n_pairs = (int64_t)nonempty;
+    ctx->n_residues = total;
+    ctx->max_len = maxlen;
+    ctx->units = units;
+    ctx->pair_ncols.resize(nonempty);
+    for (uint64_t p = 0; p < nonempty; ++p) ctx->pair_ncols[p] = pairs[p].ncols;
+    auto nomem = [&](const char* what) {
+        free_db(ctx);
+        ctx->err = std::string("device allocation failed: ") + what;
+        return SW_ERR_NOMEM;
+    };
+    if (dev_alloc(&ctx->d_db, units) != cudaSuccess) return nomem("db");
+    if (dev_alloc(&ctx->d_pairs, npairs_all) != cudaSuccess) return nomem("pairs");
+    if (dev_alloc(&ctx->d_perm, n) != cudaSuccess) return nomem("perm");
+    if (dev_alloc(&ctx->d_bnd, units * 16) != cudaSuccess) return nomem("boundary rows");
+    if (dev_alloc(&ctx->d_scores, n + 1) != cudaSuccess) return nomem("scores");
+    if (dev_alloc(&ctx->d_scores_rec, n + 1) != cudaSuccess) return nomem("scores");
+    if (dev_alloc(&ctx->d_ovf, n + 1) != cudaSuccess) return nomem("overflow list");
+    const size_t nblk = (n + kTopkKeys - 1) / kTopkKeys + 1;
+    if (dev_alloc(&ctx->d_keys[0], nblk * kMaxTopK) != cudaSuccess) return nomem("keys");
+    if (dev_alloc(&ctx->d_keys[1], nblk * kMaxTopK) != cudaSuccess) return nomem("keys");
+    SW_CUDA(ctx, cudaMemcpy(ctx->d_db, stream.data(), stream.size() ? stream.size() : 1,
+                            cudaMemcpyHostToDevice));
+    if (npairs_all)
+        SW_CUDA(ctx, cudaMemcpy(ctx->d_pairs, pairs.data(), npairs_all * sizeof(Pair2),
+                                cudaMemcpyHostToDevice));
+    if (n) SW_CUDA(ctx, cudaMemcpy(ctx->d_perm, perm.data(), n * sizeof(uint32_t),
+                                   cudaMemcpyHostToDevice));
+    ctx->db_bytes = units * 16 + npairs_all * sizeof(Pair2) + n * 4 + units * 16 * 8;
+    ctx->db_loaded = true;
+    return SW_OK;
+}
+
+extern "C" sw_status sw_db_stats_get(const sw_ctx* ctx, sw_db_stats* out) {
+    if (!ctx || !out) return SW_ERR_INVALID;
+    out->n_records = (uint64_t)ctx->n_records;
+    out->n_residues = ctx->n_residues;
+    out->n_pairs = (uint64_t)ctx->n_pairs;
+    out->max_length = ctx->max_len;
+    out->device_bytes = ctx->db_bytes;
+    return SW_OK;
+}
+
+// ---------------------------------------------------------------------------
+// kernel shape selection
+// ---------------------------------------------------------------------------
+
+namespace swb {
+
+// Blocks per SM for a shape at a query length (0 = does not fit).
+int shape_occupancy(sw_ctx* ctx, const WfKernel& k, int qlen) {
+    const size_t smem = k.smem(qlen);
+    if (smem > (size_t)ctx->max_smem) return 0;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k.fn, k.block, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return nb;
+}
+
+// Modelled cost of running pairs [b, e) with a shape: DPX-pipe instructions
+// (about 6.75 per cell pair plus ~20 per thread step) spread over the warps
+// the SM can keep resident, plus the wavefront fill of T-1 steps per pass.
+double shape_cost(sw_ctx* ctx, const WfKernel& k, int qlen, int64_t b, int64_t e) {
+    const int occ = shape_occupancy(ctx, k, qlen);
+    if (occ == 0 || e <= b) return occ == 0 ? 1e300 : 0.0;
+    const double P = (qlen + k.T * k.R - 1) / (k.T * k.R);
+    double cols = 0;
+    for (int64_t p = b; p < e; ++p) cols += ctx->pair_ncols[p] + k.T - 1;
+    const double instr = P * cols * k.T * (6.75 * k.R + 20.0);
+    const double warps = (double)occ * k.block / 32.0;
+    const double eff = std::min(1.0, warps / 12.0);
+    return instr / eff;
+}
+
+sw_kernel_config choose_config(sw_ctx* ctx, int qlen) {
+    if (ctx->has_override) return ctx->override_cfg;
+    int n = 0;
+    const WfKernel* ks = wf_kernels(&n);
+    // evaluate on a sample of pairs to keep this cheap on big DBs
+    const int64_t np = ctx->n_pairs;
+    double best = 1e301;
+    sw_kernel_config cfg{32, 32, 32, 32, 0};
+    for (int i = 0; i < n; ++i) {
+        const double c = shape_cost(ctx, ks[i], qlen, 0, np);
+        if (c < best) {
+            best = c;
+            cfg = sw_kernel_config{ks[i].T, ks[i].R, ks[i].T, ks[i].R, 0};
+        }
+    }
+    return cfg;
+}
+
+}  // namespace swb
+
+extern "C" sw_status sw_set_kernel_config(sw_ctx* ctx, const sw_kernel_config* cfg) {
+    if (!ctx) return SW_ERR_INVALID;
+    if (!cfg) {
+        ctx->has_override = false;
+        return SW_OK;
+    }
+    if (!find_kernel(cfg->long_group_width, cfg->long_rows_per_thread) ||
+        !find_kernel(cfg->short_group_width, cfg->short_rows_per_thread) || cfg->cutover < 0)
+        SW_SET(ctx, SW_ERR_INVALID, "no compiled kernel for shape %dx%d / %dx%d",
+               cfg->long_group_width, cfg->long_rows_per_thread, cfg->short_group_width,
+               cfg->short_rows_per_thread);
+    ctx->override_cfg = *cfg;
+    ctx->has_override = true;
+    return SW_OK;
+}
+
+extern "C" sw_status sw_get_kernel_config(sw_ctx* ctx, uint32_t qlen, sw_kernel_config* cfg) {
+    if (!ctx || !cfg) return SW_ERR_INVALID;
+    if (!ctx->db_loaded) SW_SET(ctx, SW_ERR_STATE, "no DB loaded");
+    *cfg = choose_config(ctx, (int)std::max<uint32_t>(qlen, 1));
+    return SW_OK;
+}
+
+extern "C" sw_status sw_get_run_stats(const sw_ctx* ctx, sw_run_stats* out) {
+    if (!ctx || !out) return SW_ERR_INVALID;
+    *out = ctx->stats;
+    return SW_OK;
+}
+
+// ---------------------------------------------------------------------------
+// search
+// ---------------------------------------------------------------------------
+
+namespace swb {
+
+// Enqueues the whole device sequence of one plain search on ctx->stream:
+// first pass (one or two shapes), 32-bit re-score, top-k rounds.  The query
+// must already be in d_query.  Returns the buffer holding the final k keys.
+sw_status take_marks(sw_ctx* ctx, sw_ctx::Marks* m) {
+    if (!ctx->spare.empty()) {
+        *m = ctx->spare.back();
+        ctx->spare.pop_back();
+        return SW_OK;
+    }
+    for (auto& e : m->e) SW_CUDA(ctx, cudaEventCreate(&e));
+    return SW_OK;
+}
+
+sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t* d_scores_rec,
+                         unsigned long long** keys_final, uint32_t* launches) {
+    cudaStream_t st = ctx->stream;
+    const sw_kernel_config cfg = choose_config(ctx, qlen);
+    ctx->stats.used = cfg;
+    *launches = 0;
+    sw_ctx::Marks mk{};
+    sw_status ms = take_marks(ctx, &mk);
+    if (ms != SW_OK) return ms;
+    mk.fp_launches = 0;
+    mk.cells = (uint64_t)qlen * ctx->n_residues;
+    SW_CUDA(ctx, cudaEventRecord(mk.e[0], st));
+    SW_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 16 * sizeof(int), st));
+    SW_CUDA(ctx, cudaMemsetAsync(ctx->d_scores, 0, (size_t)(ctx->n_records + 1) * sizeof(int), st));
+    SW_CUDA(ctx, cudaEventRecord(mk.e[1], st));
+    // pairs [0, n_long) are longer than the cut-over
+    int64_t n_long = ctx->n_pairs;
+    if (cfg.cutover > 0) {
+        n_long = 0;
+        while (n_long < ctx->n_pairs && (int)ctx->pair_ncols[n_long] > cfg.cutover) ++n_long;
+    }
+    struct Seg {
+        int T, R;
+        int64_t b, e;
+        int counter;
+    } segs[2] = {{cfg.long_group_width, cfg.long_rows_per_thread, 0, n_long, 0},
+                 {cfg.short_group_width, cfg.short_rows_per_thread, n_long, ctx->n_pairs, 1}};
+    const int ovf_thresh = 32767 - std::max(ctx->max_score, 1) + 1;
+    for (const Seg& sg : segs) {
+        if (sg.e <= sg.b) continue;
+        const WfKernel* k = find_kernel(sg.T, sg.R);
+        if (!k) SW_SET(ctx, SW_ERR_INVALID, "no kernel %dx%d", sg.T, sg.R);
+        const int occ = shape_occupancy(ctx, *k, qlen);
+        if (occ == 0)
+            SW_SET(ctx, SW_ERR_UNSUPPORTED,
+                   "query of %d residues does not fit shape %dx%d (profile %zu bytes)", qlen,
+                   sg.T, sg.R, k->smem(qlen));
+        WfArgs a;
+        a.db = ctx->d_db;
+        a.pairs = ctx->d_pairs;
+        a.pair_begin = (int)sg.b;
+        a.pair_count = (int)(sg.e - sg.b);
+        a.query = d_query;
+        a.qlen = qlen;
+        a.mat = ctx->d_mat;
+        a.neg_oe = (uint32_t)(uint16_t)(int16_t)(-(ctx->params.gap_open + ctx->params.gap_extend));
+        a.neg_oe |= a.neg_oe << 16;
+        a.neg_e = (uint32_t)(uint16_t)(int16_t)(-ctx->params.gap_extend);
+        a.neg_e |= a.neg_e << 16;
+        a.counter = ctx->d_counters + sg.counter;
+        a.bnd = ctx->d_bnd;
+        a.scores = ctx->d_scores;
+        a.n_records = (int)ctx->n_records;
+        a.ovf_list = ctx->d_ovf;
+        a.ovf_count = ctx->d_counters + 2;
+        a.ovf_thresh = ovf_thresh;
+        const int64_t groups_needed = (sg.e - sg.b);
+        int64_t grid = (int64_t)occ * ctx->num_sms;
+        const int64_t groups_per_block = k->block / k->T;
+        grid = std::min<int64_t>(grid, (groups_needed + groups_per_block - 1) / groups_per_block);
+        grid = std::max<int64_t>(grid, 1);
+        void* args[] = {&a};
+        SW_CUDA(ctx, cudaLaunchKernel(k->fn, dim3((unsigned)grid), dim3(k->block), args,
+                                      k->smem(qlen), st));
+        ++*launches;
+        ++mk.fp_launches;
+    }
+    SW_CUDA(ctx, cudaEventRecord(mk.e[2], st));
+    {
+        RescoreArgs r;
+        r.db = ctx->d_db;
+        r.pairs = ctx->d_pairs;
+        r.query = d_query;
+        r.qlen = qlen;
+        r.mat = ctx->d_mat;
+        r.gap_oe = ctx->params.gap_open + ctx->params.gap_extend;
+        r.gap_e = ctx->params.gap_extend;
+        r.ovf_list = ctx->d_ovf;
+        r.ovf_count = ctx->d_counters + 2;
+        r.bnd = ctx->d_bnd;
+        r.scores = ctx->d_scores;
+        void* args[] = {&r};
+        SW_CUDA(ctx, cudaLaunchKernel((const void*)sw_rescore32, dim3(ctx->num_sms), dim3(256),
+                                      args, 0, st));
+        ++*launches;
+    }
+    // top-k rounds: n -> ceil(n/4096)*k -> ... -> k
+    const int k = ctx->params.top_k;
+    long long n = ctx->n_records;
+    int buf = 0;
+    const unsigned long long* keys_in = nullptr;
+    bool first = true;
+    while (true) {
+        const long long blocks = std::max<long long>(1, (n + kTopkKeys - 1) / kTopkKeys);
+        TopkArgs t;
+        t.scores = ctx->d_scores;
+        t.perm = ctx->d_perm;
+        t.keys_in = first ? nullptr : keys_in;
+        t.n = n;
+        t.k = k;
+        t.cap = (ctx->params.flags & SW_FLAG_REFERENCE_CAP) ? 1 : 0;
+        t.scores_by_record = first ? d_scores_rec : nullptr;
+        t.keys_out = ctx->d_keys[buf];
+        void* args[] = {&t};
+        SW_CUDA(ctx, cudaLaunchKernel((const void*)sw_topk_round, dim3((unsigned)blocks),
+                                      dim3(kTopkThreads), args, 0, st));
+        ++*launches;
+        keys_in = ctx->d_keys[buf];
+        buf ^= 1;
+        first = false;
+        if (blocks == 1) break;
+        n = blocks * (long long)k;
+    }
+    *keys_final = const_cast<unsigned long long*>(keys_in);
+    SW_CUDA(ctx, cudaEventRecord(mk.e[3], st));
+    mk.launches = *launches;
+    ctx->pending.push_back(mk);
+    return SW_OK;
+}
+
+// Waits for the stream and folds the pending searches' event timings into
+// the totals; returns the last search's (whole, first pass) device times.
+sw_status drain(sw_ctx* ctx, float* last_ms, float* last_fp_ms) {
+    SW_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    for (auto& m : ctx->pending) {
+        float whole = 0.f, fp = 0.f;
+        SW_CUDA(ctx, cudaEventElapsedTime(&whole, m.e[0], m.e[3]));
+        SW_CUDA(ctx, cudaEventElapsedTime(&fp, m.e[1], m.e[2]));
+        ctx->totals.search_ms += whole;
+        ctx->totals.first_pass_ms += fp;
+        ctx->totals.first_pass_launches += m.fp_launches;
+        ctx->totals.launches += m.launches;
+        ctx->totals.cells += m.cells;
+        ctx->totals.queries += 1;
+        if (last_ms) *last_ms = whole;
+        if (last_fp_ms) *last_fp_ms = fp;
+        ctx->spare.push_back(m);
+    }
+    ctx->pending.clear();
+    return SW_OK;
+}
+
+sw_status ensure_query_buffers(sw_ctx* ctx, size_t qlen) {
+    if (qlen <= ctx->query_cap) return SW_OK;
+    size_t cap = std::max<size_t>(qlen, 4096);
+    dev_free(ctx->d_query);
+    if (ctx->h_query) cudaFreeHost(ctx->h_query);
+    ctx->h_query = nullptr;
+    ctx->query_cap = 0;
+    if (dev_alloc(&ctx->d_query, cap) != cudaSuccess) SW_SET(ctx, SW_ERR_NOMEM, "query buffer");
+    if (cudaMallocHost((void**)&ctx->h_query, cap) != cudaSuccess)
+        SW_SET(ctx, SW_ERR_NOMEM, "pinned query buffer");
+    if (!ctx->h_keys && cudaMallocHost((void**)&ctx->h_keys, kMaxTopK * sizeof(unsigned long long)) !=
+                            cudaSuccess)
+        SW_SET(ctx, SW_ERR_NOMEM, "pinned key buffer");
+    ctx->query_cap = cap;
+    return SW_OK;
+}
+
+}  // namespace swb
+
+extern "C" sw_status sw_search(sw_ctx* ctx, const uint8_t* query, uint32_t qlen, sw_hit* hits,
+                               uint32_t* n_hits, int32_t* scores) {
+    if (!ctx) return SW_ERR_INVALID;
+    if (!ctx->db_loaded) SW_SET(ctx, SW_ERR_STATE, "no DB loaded (call sw_db_load first)");
+    if ((qlen && !query) || (!hits && ctx->params.top_k > 0) || !n_hits)
+        SW_SET(ctx, SW_ERR_INVALID, "null argument");
+    const double t0 = now_ms();
+    const int k = ctx->params.top_k;
+    for (int i = 0; i < k; ++i) hits[i] = sw_hit{0, 0, 0};
+    *n_hits = 0;
+    ctx->stats = sw_run_stats{};
+    if (qlen == 0 || ctx->n_records == 0) {
+        if (scores) memset(scores, 0, (size_t)ctx->n_records * sizeof(int32_t));
+        ctx->stats.total_ms = now_ms() - t0;
+        return SW_OK;
+    }
+    for (uint32_t i = 0; i < qlen; ++i)
+        if (query[i] > 24) SW_SET(ctx, SW_ERR_INVALID, "query code %d at %u", query[i], i);
+    SW_CUDA(ctx, cudaSetDevice(ctx->device));
+    sw_status st = ensure_query_buffers(ctx, qlen);
+    if (st != SW_OK) return st;
+    memcpy(ctx->h_query, query, qlen);
+    SW_CUDA(ctx, cudaMemcpyAsync(ctx->d_query, ctx->h_query, qlen, cudaMemcpyHostToDevice,
+                                 ctx->stream));
+    unsigned long long* keys = nullptr;
+    uint32_t launches = 0;
+    st = enqueue_search(ctx, ctx->d_query, (int)qlen, scores ? ctx->d_scores_rec : nullptr, &keys,
+                        &launches);
+    if (st != SW_OK) return st;
+    SW_CUDA(ctx, cudaMemcpyAsync(ctx->h_keys, keys, (size_t)k * sizeof(unsigned long long),
+                                 cudaMemcpyDeviceToHost, ctx->stream));
+    if (scores)
+        SW_CUDA(ctx, cudaMemcpyAsync(scores, ctx->d_scores_rec,
+                                     (size_t)ctx->n_records * sizeof(int32_t),
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+    float kms = 0.f, fpms = 0.f;
+    st = drain(ctx, &kms, &fpms);
+    if (st != SW_OK) return st;
+    SW_CUDA(ctx, cudaGetLastError());
+    uint32_t m = 0;
+    for (int i = 0; i < k; ++i) {
+        const unsigned long long key = ctx->h_keys[i];
+        if (key == 0ull) break;
+        hits[m].score = (int32_t)(key >> 32);
+        hits[m].reserved = 0;
+        hits[m].index = 0xffffffffull - (key & 0xffffffffull);
+        ++m;
+    }
+    *n_hits = m;
+    int rescored = 0;
+    cudaMemcpy(&rescored, ctx->d_counters + 2, sizeof(int), cudaMemcpyDeviceToHost);
+    ctx->stats.kernel_ms = kms;
+    ctx->stats.first_pass_ms = fpms;
+    ctx->stats.cells = (uint64_t)qlen * ctx->n_residues;
+    ctx->stats.rescored = (uint64_t)rescored;
+    ctx->stats.launches = launches;
+    ctx->stats.queries = 1;
+    ctx->stats.total_ms = now_ms() - t0;
+    return SW_OK;
+}
+
+extern "C" sw_status sw_search_device(sw_ctx* ctx, const uint8_t* d_query, uint32_t qlen,
+                                      int32_t* d_scores) {
+    if (!ctx) return SW_ERR_INVALID;
+    if (!ctx->db_loaded) SW_SET(ctx, SW_ERR_STATE, "no DB loaded (call sw_db_load first)");
+    if (!d_query || qlen == 0) SW_SET(ctx, SW_ERR_INVALID, "empty query");
+    SW_CUDA(ctx, cudaSetDevice(ctx->device));
+    ctx->stats = sw_run_stats{};
+    unsigned long long* keys = nullptr;
+    uint32_t launches = 0;
+    sw_status st = enqueue_search(ctx, d_query, (int)qlen, d_scores, &keys, &launches);
+    if (st != SW_OK) return st;
+    ctx->stats.cells = (uint64_t)qlen * ctx->n_residues;
+    ctx->stats.launches = launches;
+    ctx->stats.queries = 1;
+    return SW_OK;
+}
+
+extern "C" sw_status sw_set_stream(sw_ctx* ctx, void* cuda_stream) {
+    if (!ctx) return SW_ERR_INVALID;
+    SW_CUDA(ctx, cudaSetDevice(ctx->device));
+    sw_status st = drain(ctx, nullptr, nullptr);
+    if (st != SW_OK) return st;
+    ctx->stream = cuda_stream ? (cudaStream_t)cuda_stream : ctx->own_stream;
+    return SW_OK;
+}
+
+extern "C" sw_status sw_sync(sw_ctx* ctx) {
+    if (!ctx) return SW_ERR_INVALID;
+    SW_CUDA(ctx, cudaSetDevice(ctx->device));
+    sw_status st = drain(ctx, nullptr, nullptr);
+    if (st != SW_OK) return st;
+    SW_CUDA(ctx, cudaGetLastError());
+    return SW_OK;
+}
+
+extern "C" sw_status sw_reset_totals(sw_ctx* ctx) {
+    if (!ctx) return SW_ERR_INVALID;
+    sw_status st = sw_sync(ctx);
+    ctx->totals = sw_totals{};
+    return st;
+}
+
+extern "C" sw_status sw_get_totals(const sw_ctx* ctx, sw_totals* out) {
+    if (!ctx || !out) return SW_ERR_INVALID;
+    *out = ctx->totals;
+    return SW_OK;
+}

@@ -1,0 +1,62 @@
+// sw_engine.h -- the context behind the C ABI's opaque sw_ctx.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/swb200.h"
+#include "sw_device.cuh"
+
+struct sw_ctx {
+    int device = 0;
+    int num_sms = 0;
+    int max_smem = 0;
+    cudaStream_t stream = nullptr;       // stream in use
+    cudaStream_t own_stream = nullptr;   // the context's own stream
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // timing events of enqueued searches: begin, first pass begin/end, end
+    struct Marks {
+        cudaEvent_t e[4];
+        uint32_t fp_launches;
+        uint32_t launches;
+        uint64_t cells;
+    };
+    std::vector<Marks> pending;
+    std::vector<Marks> spare;
+    sw_totals totals{};
+    sw_params params{};
+    int max_score = 0;
+    int8_t* d_mat = nullptr;           // 32x32 int8, codes >= 24 zeroed
+    int* d_counters = nullptr;         // [0],[1] pair counters, [2] overflow count
+
+    // resident DB
+    bool db_loaded = false;
+    int64_t n_records = 0;
+    int64_t n_pairs = 0;               // pairs with at least one column
+    uint64_t n_residues = 0;
+    uint64_t max_len = 0;
+    uint64_t units = 0;                // 16-byte units of the column stream
+    uint64_t db_bytes = 0;
+    std::vector<uint32_t> pair_ncols;  // host copy, for shape selection
+    uint4* d_db = nullptr;
+    swb::Pair2* d_pairs = nullptr;
+    uint32_t* d_perm = nullptr;        // sorted position -> record
+    uint2* d_bnd = nullptr;            // boundary rows between query passes
+    int* d_scores = nullptr;           // per sorted position
+    int* d_scores_rec = nullptr;       // per record
+    int* d_ovf = nullptr;              // overflow list
+    unsigned long long* d_keys[2] = {nullptr, nullptr};
+
+    // per-query buffers
+    size_t query_cap = 0;
+    uint8_t* d_query = nullptr;
+    uint8_t* h_query = nullptr;        // pinned
+    unsigned long long* h_keys = nullptr;  // pinned
+
+    bool has_override = false;
+    sw_kernel_config override_cfg{};
+    sw_run_stats stats{};
+    std::string err;
+};

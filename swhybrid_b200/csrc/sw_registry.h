@@ -1,0 +1,18 @@
+// sw_registry.h -- table of compiled first-pass kernel shapes.
+#pragma once
+#include <cstddef>
+
+namespace swb {
+
+struct WfKernel {
+    int T;                         // threads per record pair
+    int R;                         // query rows per thread
+    int block;                     // threads per block
+    const void* fn;                // __global__ sw_wavefront<T, R, block>
+    size_t (*smem)(int qlen);      // shared-memory bytes for a query length
+};
+
+// All instantiated shapes (sw_wf_t*.cu).
+const WfKernel* wf_kernels(int* n);
+
+}  // namespace swb

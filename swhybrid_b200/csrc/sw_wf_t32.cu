@@ -1,0 +1,19 @@
+// First-pass kernel instantiations for groups of 32 thread(s) per record pair.
+#include "sw_wavefront.cuh"
+#include "sw_registry.h"
+
+namespace swb {
+namespace {
+template <int R, int B>
+constexpr WfKernel inst() {
+    return WfKernel{32, R, B, (const void*)&sw_wavefront<32, R, B>, &wf_smem_bytes<32, R>};
+}
+}  // namespace
+
+extern const WfKernel wf_table_t32[] = {
+    inst<8, 768>(),  inst<16, 768>(), inst<24, 512>(), inst<32, 512>(),
+    inst<40, 384>(), inst<48, 384>(), inst<56, 256>(), inst<64, 256>(),
+};
+extern const int wf_table_t32_n = sizeof(wf_table_t32) / sizeof(wf_table_t32[0]);
+
+}  // namespace swb

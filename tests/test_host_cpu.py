@@ -1,0 +1,76 @@
+"""CPU tests of the host side: parameters/encoding mirror, the workload
+generators, and that libswb200.so loads and exports every C-ABI symbol of
+include/swb200.h (no compute calls without a GPU)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from swhybrid_b200 import capi, param, synth
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    src = open(os.path.join(ROOT, "include", "swb200.h")).read()
+    decl = r"^(?:const\s+)?(?:struct\s+)?[a-z_0-9]+\s*\**\s*(sw_[a-z0-9_]+)\s*\("
+    return sorted(set(re.findall(decl, src, flags=re.M)))
+
+
+def test_header_and_binding_agree():
+    assert header_symbols() == sorted(capi.EXPORTS)
+
+
+def test_library_exports_every_symbol():
+    lib = ctypes.CDLL(capi.LIB_PATH)
+    for name in header_symbols():
+        assert hasattr(lib, name), name
+
+
+def test_params_default_is_reference_param():
+    L = capi.load()
+    p = capi.sw_params()
+    L.sw_params_default(ctypes.byref(p))
+    assert (p.gap_open, p.gap_extend, p.top_k) == (10, 2, 10)
+    np.testing.assert_array_equal(np.array(p.matrix[:]).reshape(32, 32), param.blosum62())
+    ref = param.Param(["swhybrid", "-o", "11", "-e", "1", "-t", "5"])
+    assert (ref.gapOpen, ref.gapExtend, ref.topNum, ref.gapOE) == (11, 1, 5, 12)
+
+
+def test_encode_matches_python_table():
+    L = capi.load()
+    letters = b"ACDEFGHIKLMNPQRSTVWYBXZ@JOU*acdwxyz-"
+    out = (ctypes.c_uint8 * len(letters))()
+    assert L.sw_encode(letters, len(letters), out) == 0
+    np.testing.assert_array_equal(np.frombuffer(bytes(out), dtype=np.uint8),
+                                  param.encode(letters))
+    assert param.encode("ABZ@J").tolist() == [0, 1, 22, 23, 24]
+
+
+def test_no_device_is_reported_not_faked():
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("GPU present")
+    except Exception:
+        pass
+    with pytest.raises(capi.SwError) as e:
+        capi.Context(0)
+    assert e.value.status in (9, 2)
+
+
+def test_generators_are_seeded_and_shaped():
+    a = synth.small_db(1, 2000)
+    b = synth.small_db(1, 2000)
+    assert np.array_equal(a.residues, b.residues)
+    L = a.lengths()
+    assert L.min() >= 20 and L.max() <= 5000
+    assert abs(np.median(L) - np.exp(5.6)) < 30
+    # background composition close to the table
+    counts = np.bincount(a.residues, minlength=23) / a.total
+    assert abs(counts[param.ALPHABET.index("L")] - 0.09019) < 0.01
+    assert counts[param.ALPHABET.index("B")] == 0
+    sweep = synth.sweep_lengths()
+    assert sweep[0] == 144 and sweep[-1] == 5478 and len(sweep) == 20

@@ -1,0 +1,170 @@
+"""GPU parity of the plain search path, through the C ABI (libswb200.so).
+
+Every record's score must equal the reference's (its own AVX2 int8 kernel +
+RecalcWorker int16 pass, as stored in tests/golden/ by make_golden.py, or the
+oracle restatement pinned to those vectors), bit for bit; top-k must equal the
+oracle's under the stated tie order (score descending, record index
+ascending)."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from swhybrid_b200 import capi, param, synth
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+M = param.blosum62()
+
+
+def load(name):
+    z = np.load(os.path.join(GOLD, name + ".npz"))
+    qo = z["qoffsets"].astype(np.int64)
+    queries = [z["queries"][qo[i]:qo[i + 1]] for i in range(len(qo) - 1)]
+    return z["residues"], z["offsets"], queries, z["scores"]
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = capi.Context(0, capi.default_params(top_k=10))
+    yield c
+    c.close()
+
+
+def check_topk(hits, scores, k=10):
+    sc, idx = oracle.topk(scores, k)
+    assert [h[0] for h in hits] == sc.tolist()
+    assert [h[1] for h in hits] == idx.tolist()
+
+
+@pytest.mark.parametrize("name", ["edge", "homolog", "saturation"])
+def test_golden_sets_bit_exact(ctx, name):
+    res, off, queries, gold = load(name)
+    ctx.load_db(res, off)
+    for qi, q in enumerate(queries):
+        hits, scores = ctx.search(q, want_scores=True)
+        np.testing.assert_array_equal(scores, gold[qi], err_msg=f"{name} query {qi} len {len(q)}")
+        check_topk(hits, gold[qi])
+
+
+def test_small20k_query375_bit_exact(ctx):
+    z = np.load(os.path.join(GOLD, "small20k_q375.npz"))
+    db = synth.small_db(1, 20_000)
+    q = synth.query(375, 375)
+    ctx.load_db(db.residues, db.offsets)
+    hits, scores = ctx.search(q, want_scores=True)
+    np.testing.assert_array_equal(scores, z["scores"])
+    check_topk(hits, z["scores"])
+
+
+def all_shapes(ctx):
+    """Every compiled (group width, rows per thread) shape."""
+    shapes = []
+    for T in (1, 2, 4, 8, 16, 32):
+        for R in (8, 16, 24, 32, 40, 48, 56, 64):
+            shapes.append((T, R))
+    return shapes
+
+
+def test_every_kernel_shape_bit_exact(ctx):
+    res, off, queries, gold = load("homolog")
+    ctx.load_db(res, off)
+    try:
+        for T, R in all_shapes(ctx):
+            ctx.set_kernel_config((T, R, T, R, 0))
+            for qi in (0, 1):
+                _, scores = ctx.search(queries[qi], want_scores=True)
+                np.testing.assert_array_equal(scores, gold[qi], err_msg=f"shape {T}x{R} q{qi}")
+    finally:
+        ctx.set_kernel_config(None)
+
+
+def test_cutover_split_bit_exact(ctx):
+    res, off, queries, gold = load("homolog")
+    ctx.load_db(res, off)
+    try:
+        for cfg in [(32, 32, 4, 16, 400), (16, 24, 1, 32, 1000), (8, 64, 2, 40, 200)]:
+            ctx.set_kernel_config(cfg)
+            for qi in (0, 1):
+                _, scores = ctx.search(queries[qi], want_scores=True)
+                np.testing.assert_array_equal(scores, gold[qi], err_msg=f"config {cfg}")
+    finally:
+        ctx.set_kernel_config(None)
+
+
+def test_int16_threshold_and_int32_pass():
+    """Scores around the 16-bit overflow threshold and above 65535: the 32-bit
+    re-score must be exact; the reference cap reports 65535."""
+    res, off, queries, gold = load("saturation")
+    with capi.Context(0, capi.default_params(reference_cap=False)) as c:
+        c.load_db(res, off)
+        L = np.diff(off.astype(np.int64))
+        for q in queries:
+            _, scores = c.search(q, want_scores=True)
+            np.testing.assert_array_equal(scores, 11 * np.minimum(L, len(q)))
+        st = c.run_stats()
+        assert st.rescored > 0
+
+
+def test_long_records_and_many_passes(ctx):
+    """Records up to 12,000 residues and a 3,000-residue query (several
+    passes for every shape) against the oracle."""
+    rng = np.random.default_rng(21)
+    q = synth.residues(rng, 3000)
+    lens = np.concatenate([rng.integers(8000, 12000, size=6), rng.integers(1, 400, size=50)])
+    db = synth.db_from_lengths(rng, lens)
+    db, _ = synth.plant_homologs(rng, db, q, 0.05)
+    want = oracle.search(q, db.residues, db.offsets, M, 12, 2, mode=1)
+    ctx.load_db(db.residues, db.offsets)
+    hits, scores = ctx.search(q, want_scores=True)
+    np.testing.assert_array_equal(scores, want)
+    check_topk(hits, want)
+
+
+def test_other_gap_costs_match_oracle():
+    rng = np.random.default_rng(22)
+    db = synth.small_db(5, 800)
+    q = synth.residues(rng, 300)
+    for go, ge in [(11, 1), (5, 3), (0, 1)]:
+        with capi.Context(0, capi.default_params(gap_open=go, gap_extend=ge, reference_cap=False)) as c:
+            c.load_db(db.residues, db.offsets)
+            _, scores = c.search(q, want_scores=True)
+        want = oracle.search(q, db.residues, db.offsets, M, go + ge, ge, mode=0)
+        np.testing.assert_array_equal(scores, want, err_msg=f"gaps {go}/{ge}")
+
+
+def test_deterministic_and_order_invariant(ctx):
+    db = synth.small_db(7, 3000)
+    q = synth.query(8, 500)
+    ctx.load_db(db.residues, db.offsets)
+    h1, s1 = ctx.search(q, want_scores=True)
+    h2, s2 = ctx.search(q, want_scores=True)
+    assert h1 == h2
+    np.testing.assert_array_equal(s1, s2)
+    perm = np.random.default_rng(1).permutation(db.n)
+    sub = db.subset(perm)
+    ctx.load_db(sub.residues, sub.offsets)
+    _, s3 = ctx.search(q, want_scores=True)
+    np.testing.assert_array_equal(s3, s1[perm])
+
+
+def test_empty_inputs(ctx):
+    res = np.zeros(0, dtype=np.uint8)
+    ctx.load_db(res, np.zeros(4, dtype=np.uint64))        # three empty records
+    hits, scores = ctx.search(synth.query(1, 50), want_scores=True)
+    assert hits == [] and scores.tolist() == [0, 0, 0]
+    db = synth.small_db(2, 100)
+    ctx.load_db(db.residues, db.offsets)
+    hits, scores = ctx.search(np.zeros(0, dtype=np.uint8), want_scores=True)
+    assert hits == [] and not scores.any()
+
+
+def test_bad_codes_rejected(ctx):
+    db = synth.small_db(2, 100)
+    ctx.load_db(db.residues, db.offsets)
+    bad = synth.query(1, 50)
+    bad[3] = 40
+    with pytest.raises(capi.SwError) as e:
+        ctx.search(bad)
+    assert e.value.status == 1
