@@ -48,6 +48,7 @@ WORKLOADS = {
     "full": "plain method, full size: 570,000+200 records (~205M residues), "
             "20 query lengths log-spaced 144..5,478, one query per call",
     "small": "plain method, small: 20,000 records (~6.5M residues), query 375",
+    "profile": "profiling case: the full-size DB (~205M residues) and one query of 1,434",
 }
 
 
@@ -64,6 +65,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--config", type=str, default=None,
                     help="force a kernel shape 'T,R,T,R,cutover'")
+    ap.add_argument("--kernel-only", action="store_true",
+                    help="time the resident path only (no e2e, probe or CPU baseline)")
     return ap.parse_args()
 
 
@@ -72,6 +75,9 @@ def make_workload(name: str, rank: int):
     if name == "small":
         db = synth.small_db(1, 20_000)
         queries = [synth.query(375, 375)]
+    elif name == "profile":
+        db = synth.full_db(2 + 1000 * rank)
+        queries = [synth.query(112, 1434)]
     else:
         db = synth.full_db(2 + 1000 * rank)
         queries = [synth.query(100 + i, int(L)) for i, L in enumerate(synth.sweep_lengths())]
@@ -151,16 +157,22 @@ def probe_rates(device: int):
     L = ctypes.CDLL(path)
     L.swprobe_rates.restype = ctypes.c_int
     L.swprobe_rates.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
-    out = (ctypes.c_double * 8)()
+    out = (ctypes.c_double * 16)()
     rc = L.swprobe_rates(device, out, 4096)
     if rc != 0:
         raise RuntimeError(f"swprobe_rates failed: {rc}")
-    sms, mhz = out[4], out[5]
+    sms, mhz = out[9], out[10]
+    per = lambda v, lanes: v / lanes / 32 / (sms * mhz * 1e6)  # warp-instr / clk / SM
     return {
-        "viaddmax_s16x2_instr_per_clk_sm": out[0] / 2 / 32 / (sms * mhz * 1e6),
-        "vimax3_s16x2_instr_per_clk_sm": out[1] / 2 / 32 / (sms * mhz * 1e6),
-        "prmt_instr_per_clk_sm": out[2] / 32 / (sms * mhz * 1e6),
-        "cell_mix_gcups": out[3] / 1e9,
+        "viaddmax_s16x2_instr_per_clk_sm": per(out[0], 2),
+        "vimax3_s16x2_instr_per_clk_sm": per(out[1], 2),
+        "prmt_instr_per_clk_sm": per(out[2], 1),
+        "imad_instr_per_clk_sm": per(out[4], 1),
+        "dpx_imad_mix_instr_per_clk_sm": per(out[5], 1),
+        "iadd_instr_per_clk_sm": per(out[6], 1),
+        "lop3_instr_per_clk_sm": per(out[7], 1),
+        "cell_mix_v1_gcups": out[3] / 1e9,
+        "cell_mix_gcups": out[8] / 1e9,
         "sms": int(sms), "attr_clock_mhz": mhz,
     }
 
@@ -258,6 +270,8 @@ def run_ours(args, rank, world, local_rank):
     t0 = time.time()
     ctx.load_db(db.residues, db.offsets)
     load_s = time.time() - t0
+    from swhybrid_b200 import autotune
+    tuned = autotune.apply(ctx)
     if args.config:
         ctx.set_kernel_config(tuple(int(x) for x in args.config.split(",")))
     stream = torch.cuda.Stream(device=local_rank)
@@ -292,6 +306,15 @@ def run_ours(args, rank, world, local_rank):
     tot = ctx.totals()
     dev_ms_max = max_over_ranks(dev_ms)
     value = cells_step * args.steps * world / (dev_ms_max * 1e-3) / 1e9
+
+    if args.kernel_only:
+        if rank == 0:
+            print(json.dumps({"kernel_only": True, "value": round(value, 3), "unit": "GCUPS",
+                              "ms": round(dev_ms_max, 3),
+                              "first_pass_launches": int(tot.first_pass_launches),
+                              "config": list(ctx.kernel_config(len(queries[0])))}), flush=True)
+        ctx.close()
+        return None, db, queries
 
     # ---- timed: end to end through sw_search (host buffers) ----
     ctx.set_stream(None)
@@ -344,6 +367,7 @@ def run_ours(args, rank, world, local_rank):
                        "top_k": 10, "gaps": "open 10 / extend 2", "matrix": "BLOSUM62",
                        "l2": "inputs larger than L2 (DB column streams ~%d MB)" %
                              (st.device_bytes // 9 // 2**20),
+                       "tuning_table": "swhybrid_b200/tuned/b200.json" if tuned else "cost model",
                        "kernel_config_q144": list(ctx.kernel_config(144)),
                        "kernel_config_q5478": list(ctx.kernel_config(5478)),
                        "db_generate_s": round(gen_s, 2), "db_load_s": round(load_s, 2)},
@@ -393,11 +417,13 @@ def main():
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     line, db, queries = run_ours(args, rank, world, local_rank)
+    if line is None:
+        return 0
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb, _ = cpu_baseline(db, queries, args.cpu_seconds)
         line["cpu_baseline"] = {k: (round(v, 3) if isinstance(v, float) else v)
                                 for k, v in cb.items()}
-    if rank == 0:
+    if rank == 0 and line is not None:
         print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist

@@ -149,6 +149,16 @@ sw_status sw_search_device(struct sw_ctx *ctx, const uint8_t *d_query,
 /* Overrides the kernel shape chosen for plain searches (NULL = automatic). */
 sw_status sw_set_kernel_config(struct sw_ctx *ctx, const sw_kernel_config *cfg);
 
+/* Shape table from the autotuner: for a query of qlen residues the first
+ * entry (in the given order, sorted by max_qlen) with qlen <= max_qlen is used.
+ * n = 0 clears the table (the built-in cost model is used again). */
+typedef struct sw_tuning_entry {
+    uint32_t max_qlen;
+    sw_kernel_config cfg;
+} sw_tuning_entry;
+
+sw_status sw_set_tuning(struct sw_ctx *ctx, const sw_tuning_entry *entries, uint32_t n);
+
 /* Shape the library would pick for a query of this length. */
 sw_status sw_get_kernel_config(struct sw_ctx *ctx, uint32_t qlen, sw_kernel_config *cfg);
 

@@ -1,0 +1,121 @@
+"""Autotuner for the first-pass kernel shape (group width x rows per thread,
+and the long/short cut-over).
+
+For a DB and a list of query lengths it times every compiled shape on the
+present GPU (device time of the first-pass launches, CUDA events inside the
+library), keeps the fastest per length, and writes a JSON table that
+``apply()`` hands to the library (``sw_set_tuning``).  Shapes whose profile
+does not fit in shared memory for a length are skipped (the library refuses
+them with SW_ERR_UNSUPPORTED).
+
+    python -m swhybrid_b200.autotune --out swhybrid_b200/tuned/b200.json
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+from . import capi, synth
+
+GROUP_WIDTHS = (1, 2, 4, 8, 16, 32)
+ROWS = (8, 16, 24, 32, 40, 48, 56, 64)
+DEFAULT_TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned", "b200.json")
+
+
+def time_shape(ctx: capi.Context, dq, qlen: int, cfg: tuple, reps: int = 2) -> float | None:
+    """GCUPS of the first pass for one shape, or None if it does not fit."""
+    ctx.set_kernel_config(cfg)
+    try:
+        ctx.search_device(dq.data_ptr(), qlen)          # warm-up
+        ctx.sync()
+    except capi.SwError as e:
+        if e.status == 6:
+            return None
+        raise
+    ctx.reset_totals()
+    for _ in range(reps):
+        ctx.search_device(dq.data_ptr(), qlen)
+    ctx.sync()
+    t = ctx.totals()
+    return t.cells / (t.first_pass_ms * 1e-3) / 1e9
+
+
+def sweep(ctx: capi.Context, lengths, shapes=None, reps: int = 2, log=print):
+    import torch
+    shapes = shapes or [(T, R) for T in GROUP_WIDTHS for R in ROWS]
+    results = {}
+    for L in lengths:
+        q = synth.query(9000 + int(L), int(L))
+        dq = torch.from_numpy(q).cuda()
+        row = {}
+        for T, R in shapes:
+            g = time_shape(ctx, dq, int(L), (T, R, T, R, 0), reps)
+            if g is not None:
+                row[f"{T}x{R}"] = round(g, 1)
+        best = max(row, key=row.get)
+        results[int(L)] = {"best": best, "gcups": row[best], "all": row}
+        log(f"qlen {L}: best {best} {row[best]:.0f} GCUPS")
+    ctx.set_kernel_config(None)
+    return results
+
+
+def table_from_sweep(results) -> list:
+    """[(max_qlen, (T, R, T, R, 0)), ...]: each measured length covers the
+    lengths up to the midpoint (geometric) to the next measured length."""
+    Ls = sorted(results)
+    out = []
+    for i, L in enumerate(Ls):
+        hi = int(np.sqrt(L * Ls[i + 1])) if i + 1 < len(Ls) else 1 << 30
+        T, R = (int(x) for x in results[L]["best"].split("x"))
+        out.append((hi, (T, R, T, R, 0)))
+    return out
+
+
+def save(results, path: str = DEFAULT_TABLE, meta=None):
+    os.makedirs(os.path.dirname(path), exist_ok=True)
+    doc = {"meta": meta or {}, "sweep": {str(k): v for k, v in results.items()},
+           "table": [[hi, list(cfg)] for hi, cfg in table_from_sweep(results)]}
+    with open(path, "w") as f:
+        json.dump(doc, f, indent=1)
+
+
+def load_table(path: str = DEFAULT_TABLE):
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        doc = json.load(f)
+    return [(int(hi), tuple(int(x) for x in cfg)) for hi, cfg in doc["table"]]
+
+
+def apply(ctx: capi.Context, path: str = DEFAULT_TABLE) -> bool:
+    tab = load_table(path)
+    if not tab:
+        return False
+    ctx.set_tuning(tab)
+    return True
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=DEFAULT_TABLE)
+    ap.add_argument("--records", type=int, default=142_500)
+    ap.add_argument("--long", type=int, default=50)
+    ap.add_argument("--reps", type=int, default=2)
+    args = ap.parse_args()
+    db = synth.full_db(7, args.records, args.long)
+    ctx = capi.Context(0)
+    ctx.load_db(db.residues, db.offsets)
+    t0 = time.time()
+    res = sweep(ctx, synth.sweep_lengths(), reps=args.reps)
+    import torch
+    save(res, args.out, meta={"gpu": torch.cuda.get_device_name(0), "records": db.n,
+                              "residues": db.total, "seconds": round(time.time() - t0, 1)})
+    print("wrote", args.out)
+
+
+if __name__ == "__main__":
+    main()

@@ -28,6 +28,7 @@ EXPORTS = [
     "sw_last_error", "sw_db_load", "sw_db_stats_get", "sw_search",
     "sw_search_device", "sw_set_kernel_config", "sw_get_kernel_config",
     "sw_get_run_stats", "sw_set_stream", "sw_sync", "sw_reset_totals", "sw_get_totals",
+    "sw_set_tuning",
 ]
 
 
@@ -56,6 +57,10 @@ class sw_kernel_config(ctypes.Structure):
     def as_tuple(self):
         return (self.long_group_width, self.long_rows_per_thread, self.short_group_width,
                 self.short_rows_per_thread, self.cutover)
+
+
+class sw_tuning_entry(ctypes.Structure):
+    _fields_ = [("max_qlen", ctypes.c_uint32), ("cfg", sw_kernel_config)]
 
 
 class sw_db_stats(ctypes.Structure):
@@ -125,6 +130,8 @@ def load(path: str = LIB_PATH):
     L.sw_reset_totals.argtypes = [P]
     L.sw_get_totals.restype = ctypes.c_int
     L.sw_get_totals.argtypes = [P, ctypes.POINTER(sw_totals)]
+    L.sw_set_tuning.restype = ctypes.c_int
+    L.sw_set_tuning.argtypes = [P, ctypes.POINTER(sw_tuning_entry), ctypes.c_uint32]
     _lib = L
     return L
 
@@ -216,6 +223,14 @@ class Context:
             return
         c = sw_kernel_config(*cfg)
         self._check(self.L.sw_set_kernel_config(self.h, ctypes.byref(c)), "sw_set_kernel_config")
+
+    def set_tuning(self, table):
+        """table: [(max_qlen, (T, R, T, R, cutover)), ...] sorted by max_qlen."""
+        arr = (sw_tuning_entry * max(len(table), 1))()
+        for i, (hi, cfg) in enumerate(table):
+            arr[i].max_qlen = int(hi)
+            arr[i].cfg = sw_kernel_config(*cfg)
+        self._check(self.L.sw_set_tuning(self.h, arr, len(table)), "sw_set_tuning")
 
     def kernel_config(self, qlen: int) -> tuple:
         c = sw_kernel_config()

@@ -7,11 +7,18 @@
 //   op 0  __viaddmax_s16x2          (fused add + max, 2 x int16)
 //   op 1  __vimax3_s16x2            (3-way max, 2 x int16)
 //   op 2  prmt.b32                  (byte permute)
-//   op 3  the first pass's per-row cell recurrence (5 DPX + 1 PRMT per row
-//         and 1 three-way max per two rows), the instruction mix of
-//         sw_wavefront.cuh without its shared-memory loads and shuffles.
-// Rates are returned in lane-operations per second (ops 0-2) and in cell
-// updates per second (op 3, two cells per row and register).
+//   op 3  a per-row cell recurrence of 5 DPX + 1 PRMT per row and 1
+//         three-way max per two rows (earlier form of the first pass)
+//   op 4  mad.lo.u32 with a run-time multiplier (IMAD)
+//   op 5  __viaddmax_s16x2 and IMAD interleaved 1:1 (do they co-issue?)
+//   op 6  three-input integer add (IADD3)
+//   op 7  three-input logic op (LOP3)
+//   op 8  the first pass's per-row cell recurrence as sw_wavefront.cuh runs
+//         it (4 DPX + 1 IMAD + 1 PRMT per row, 1 three-way max per two rows),
+//         without its shared-memory loads and shuffles
+// Rates are returned in lane-operations per second (ops 0-2, 4-7; a 16x2
+// operation counts as two) and in cell updates per second (ops 3 and 8, two
+// cells per row and register).
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -20,6 +27,12 @@ namespace {
 __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
     uint32_t r;
     asm volatile("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(sel));
+    return r;
+}
+
+__device__ __forceinline__ uint32_t mad(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t r;
+    asm volatile("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
     return r;
 }
 
@@ -36,6 +49,14 @@ __global__ void __launch_bounds__(512) rate_kernel(uint32_t* sink, int iters, ui
             if (OP == 0) a[j] = __viaddmax_s16x2(a[j], b, a[j ^ 1]);
             if (OP == 1) a[j] = __vimax3_s16x2(a[j], b, a[j ^ 1]);
             if (OP == 2) a[j] = prmt(a[j], a[j ^ 1], 0xC480u + (uint32_t)j);
+            if (OP == 4) a[j] = mad(a[j], c, a[j ^ 1]);
+            if (OP == 5) a[j] = (j & 1) ? mad(a[j], c, a[j ^ 1]) : __viaddmax_s16x2(a[j], b, a[j ^ 1]);
+            if (OP == 6) {
+                uint32_t r;
+                asm volatile("add.u32 %0, %1, %2;\n\tadd.u32 %0, %0, %3;" : "=r"(r) : "r"(a[j]), "r"(a[j ^ 1]), "r"(b));
+                a[j] = r;
+            }
+            if (OP == 7) a[j] = (a[j] & a[j ^ 1]) ^ b;
         }
         b += c;
     }
@@ -87,6 +108,47 @@ __global__ void __launch_bounds__(512) cell_kernel(uint32_t* sink, int iters, ui
     if (r == 0x9e3779b9u) sink[0] = r;
 }
 
+// The first pass's cell recurrence with biased lanes (sw_wavefront.cuh rows8).
+__global__ void __launch_bounds__(512) cell2_kernel(uint32_t* sink, int iters, uint32_t seed) {
+    constexpr int R = 16;
+    uint32_t H[R], E[R];
+    const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t Z = 0x000c000cu, NQ = 0u - Z, NE = 0xfffefffeu, one = seed >> 31 | 1u;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        H[k] = Z + ((tid + k) & 0x000f000fu);
+        E[k] = Z;
+    }
+    uint32_t S = Z, f = Z, diag = Z;
+    uint32_t A0 = seed ^ tid, A1 = seed * 3u, B0 = seed + tid, B1 = ~seed;
+    for (int i = 0; i < iters; ++i) {
+#pragma unroll
+        for (int k = 0; k < R; ++k) {
+            const uint32_t wa = (k & 4) ? A1 : A0, wb = (k & 4) ? B1 : B0;
+            const uint32_t sel = (uint32_t)(k & 3) | ((uint32_t)((k & 3) | 8) << 4) |
+                                 ((uint32_t)(4 + (k & 3)) << 8) |
+                                 ((uint32_t)((4 + (k & 3)) | 8) << 12);
+            const uint32_t sc = prmt(wa, wb, sel);
+            uint32_t h = __viaddmax_s16x2(diag, sc, E[k]);
+            h = __vimax3_s16x2(h, f, Z);
+            diag = H[k];
+            H[k] = h;
+            const uint32_t hq = mad(h, one, NQ);
+            E[k] = __viaddmax_s16x2(E[k], NE, hq);
+            f = __viaddmax_s16x2(f, NE, hq);
+            if (k & 1) S = __vimax3_s16x2(S, H[k - 1], H[k]);
+        }
+        A0 = A0 * 1664525u + 1013904223u;
+        B0 ^= A0;
+        f = Z;
+        diag = (S & 0x00ff00ffu) | Z;
+    }
+    uint32_t r = S;
+#pragma unroll
+    for (int k = 0; k < R; ++k) r ^= H[k] ^ E[k];
+    if (r == 0x9e3779b9u) sink[0] = r;
+}
+
 template <typename K>
 double time_kernel(K kern, int sms, int iters, uint32_t* sink, double work_per_thread) {
     const int blocks = sms * 4, threads = 512;
@@ -108,8 +170,8 @@ double time_kernel(K kern, int sms, int iters, uint32_t* sink, double work_per_t
 
 }  // namespace
 
-// out[0..3] = rates of ops 0..3 (see the file comment); out[4] = SM count;
-// out[5] = SM clock in MHz reported by the device attribute.  Returns 0 on
+// out[0..8] = rates of ops 0..8 (see the file comment); out[9] = SM count;
+// out[10] = SM clock in MHz reported by the device attribute.  Returns 0 on
 // success.
 extern "C" int swprobe_rates(int device, double* out, int iters) {
     if (cudaSetDevice(device) != cudaSuccess) return 1;
@@ -123,8 +185,13 @@ extern "C" int swprobe_rates(int device, double* out, int iters) {
     out[1] = time_kernel(rate_kernel<1>, sms, iters, sink, 8.0 * 2);
     out[2] = time_kernel(rate_kernel<2>, sms, iters, sink, 8.0);
     out[3] = time_kernel(cell_kernel, sms, iters / 4, sink, 16.0 * 2);
-    out[4] = sms;
-    out[5] = clk / 1000.0;
+    out[4] = time_kernel(rate_kernel<4>, sms, iters, sink, 8.0);
+    out[5] = time_kernel(rate_kernel<5>, sms, iters, sink, 8.0);
+    out[6] = time_kernel(rate_kernel<6>, sms, iters, sink, 16.0);
+    out[7] = time_kernel(rate_kernel<7>, sms, iters, sink, 8.0);
+    out[8] = time_kernel(cell2_kernel, sms, iters / 4, sink, 16.0 * 2);
+    out[9] = sms;
+    out[10] = clk / 1000.0;
     cudaFree(sink);
     return cudaGetLastError() == cudaSuccess ? 0 : 3;
 }

@@ -36,15 +36,16 @@ struct WfArgs {
     const uint8_t* query;       // device query codes, qlen entries (< 25)
     int qlen;
     const int8_t* mat;          // 32x32, [query code][db code]; codes >= 24 score 0
-    uint32_t neg_oe;            // dup16(-(open+extend))
+    uint32_t bias2;             // dup16(open+extend): the biased zero of a lane
     uint32_t neg_e;             // dup16(-extend)
+    uint32_t one;               // 1 (multiplier of the IMAD subtraction)
     int* counter;               // pairs claimed (zero before the launch)
     uint2* bnd;                 // boundary rows: 16 entries per 16-byte stream unit
     int* scores;                // per sorted record position
     int n_records;
     int* ovf_list;              // sorted positions for the 32-bit pass
     int* ovf_count;
-    int ovf_thresh;             // lane value >= this may have wrapped
+    int ovf_thresh;             // biased lane value >= this may have wrapped
 };
 
 __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {

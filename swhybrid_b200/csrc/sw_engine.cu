@@ -425,6 +425,14 @@ double shape_cost(sw_ctx* ctx, const WfKernel& k, int qlen, int64_t b, int64_t e
 
 sw_kernel_config choose_config(sw_ctx* ctx, int qlen) {
     if (ctx->has_override) return ctx->override_cfg;
+    for (const sw_tuning_entry& e : ctx->tuning) {
+        if ((uint32_t)qlen > e.max_qlen) continue;
+        const WfKernel* kl = find_kernel(e.cfg.long_group_width, e.cfg.long_rows_per_thread);
+        const WfKernel* ks = find_kernel(e.cfg.short_group_width, e.cfg.short_rows_per_thread);
+        if (kl && ks && shape_occupancy(ctx, *kl, qlen) > 0 && shape_occupancy(ctx, *ks, qlen) > 0)
+            return e.cfg;
+        break;   // the tuned shape does not fit this length: fall back to the model
+    }
     int n = 0;
     const WfKernel* ks = wf_kernels(&n);
     // evaluate on a sample of pairs to keep this cheap on big DBs
@@ -456,6 +464,20 @@ extern "C" sw_status sw_set_kernel_config(sw_ctx* ctx, const sw_kernel_config* c
                cfg->short_rows_per_thread);
     ctx->override_cfg = *cfg;
     ctx->has_override = true;
+    return SW_OK;
+}
+
+extern "C" sw_status sw_set_tuning(sw_ctx* ctx, const sw_tuning_entry* entries, uint32_t n) {
+    if (!ctx || (n && !entries)) return SW_ERR_INVALID;
+    std::vector<sw_tuning_entry> tab(entries, entries + n);
+    for (const sw_tuning_entry& e : tab)
+        if (!find_kernel(e.cfg.long_group_width, e.cfg.long_rows_per_thread) ||
+            !find_kernel(e.cfg.short_group_width, e.cfg.short_rows_per_thread) || e.cfg.cutover < 0)
+            SW_SET(ctx, SW_ERR_INVALID, "tuning entry names an uncompiled shape");
+    for (size_t i = 1; i < tab.size(); ++i)
+        if (tab[i].max_qlen < tab[i - 1].max_qlen)
+            SW_SET(ctx, SW_ERR_INVALID, "tuning entries not sorted by max_qlen");
+    ctx->tuning = std::move(tab);
     return SW_OK;
 }
 
@@ -536,8 +558,9 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
         a.query = d_query;
         a.qlen = qlen;
         a.mat = ctx->d_mat;
-        a.neg_oe = (uint32_t)(uint16_t)(int16_t)(-(ctx->params.gap_open + ctx->params.gap_extend));
-        a.neg_oe |= a.neg_oe << 16;
+        a.bias2 = (uint32_t)(ctx->params.gap_open + ctx->params.gap_extend);
+        a.bias2 |= a.bias2 << 16;
+        a.one = 1u;
         a.neg_e = (uint32_t)(uint16_t)(int16_t)(-ctx->params.gap_extend);
         a.neg_e |= a.neg_e << 16;
         a.counter = ctx->d_counters + sg.counter;

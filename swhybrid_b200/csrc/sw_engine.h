@@ -55,6 +55,7 @@ struct sw_ctx {
     uint8_t* h_query = nullptr;        // pinned
     unsigned long long* h_keys = nullptr;  // pinned
 
+    std::vector<sw_tuning_entry> tuning;
     bool has_override = false;
     sw_kernel_config override_cfg{};
     sw_run_stats stats{};

@@ -24,9 +24,11 @@
 // src/AVXKernel.cpp:196-218, with the floor at 0 made explicit):
 //   h  = max(diag + P, E, F, 0);  S = max(S, h)
 //   hq = h - (open+extend);  E = max(E - extend, hq);  F = max(F - extend, hq)
-// E, F stay >= -(open+extend) because h >= 0, so no lane underflows; a lane
-// can only wrap upward after exceeding 32767 - max(matrix), which is the
-// overflow threshold handed to the 32-bit re-score pass.
+// Lanes hold value + (open+extend) (see CellK), so every lane stays in
+// [0, 32767] and the subtraction of open+extend cannot borrow across halves; a
+// lane can only wrap upward after exceeding 32767 - max(matrix), which is the
+// overflow threshold handed to the 32-bit re-score pass.  The residue chunk
+// and the boundary row are prefetched so that no step waits on global memory.
 //
 // The query profile lives in shared memory as signed bytes, laid out so that
 // each thread's 8-row chunk for a residue code is one 8-byte word and the 16
@@ -56,24 +58,46 @@ __device__ __forceinline__ uint32_t pick_pack(const uint2& A, const uint2& B) {
     return pack_s8x2<I & 3>(I < 4 ? A.x : A.y, I < 4 ? B.x : B.y);
 }
 
-// One 8-row chunk of the cell recurrence (rows j*8 .. j*8+7 of this thread).
+// 32-bit integer multiply-add (kept as IMAD: the multiplier is a run-time 1),
+// used for the packed subtraction h - (open+extend) on lanes that are biased so
+// that no half can borrow from the other.
+__device__ __forceinline__ uint32_t mad_u32(uint32_t a, uint32_t b, uint32_t c) {
+    uint32_t r;
+    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
+    return r;
+}
+
+// Constants of the cell recurrence.  Every H/E/F/S lane holds value + B with
+// B = open+extend (so "score 0" is B): h' >= B keeps h' - (open+extend) >= 0
+// in both halves, which makes the packed subtraction an ordinary 32-bit add.
+struct CellK {
+    uint32_t bias2;     // (B, B)
+    uint32_t neg_q2;    // -(B << 16 | B) mod 2^32, i.e. subtract open+extend per half
+    uint32_t neg_e2;    // (-extend, -extend)
+    uint32_t one;       // 1, from a kernel argument
+};
+
+// One 8-row chunk of the cell recurrence (rows j*8 .. j*8+7 of this thread):
+//   t  = max(diag + P, E)            (DPX add+max)
+//   h  = max(t, F, B)                (DPX 3-way max; B = biased zero)
+//   hq = h - (open+extend)           (IMAD, both halves at once)
+//   E  = max(E - extend, hq), F = max(F - extend, hq)   (DPX add+max)
+//   S  = max(S, h, h_next)           (DPX 3-way max, every second row)
 template <int R, int J>
 __device__ __forceinline__ void rows8(uint32_t (&H)[R], uint32_t (&E)[R], const uint2 A,
                                       const uint2 B, uint32_t& diag, uint32_t& f,
-                                      uint32_t& S, const uint32_t NEG_OE,
-                                      const uint32_t NEG_E) {
-    const uint32_t MIN16 = 0x80008000u;
+                                      uint32_t& S, const CellK& K) {
 #define SWB_CELL(I)                                                          \
     {                                                                        \
         constexpr int k = J * 8 + I;                                         \
         const uint32_t sc = pick_pack<I>(A, B);                              \
-        uint32_t h = __viaddmax_s16x2_relu(diag, sc, E[k]);                  \
-        h = __vimax_s16x2_relu(h, f);                                        \
+        uint32_t h = __viaddmax_s16x2(diag, sc, E[k]);                       \
+        h = __vimax3_s16x2(h, f, K.bias2);                                   \
         diag = H[k];                                                         \
         H[k] = h;                                                            \
-        const uint32_t hq = __viaddmax_s16x2(h, NEG_OE, MIN16);              \
-        E[k] = __viaddmax_s16x2(E[k], NEG_E, hq);                            \
-        f = __viaddmax_s16x2(f, NEG_E, hq);                                  \
+        const uint32_t hq = mad_u32(h, K.one, K.neg_q2);                     \
+        E[k] = __viaddmax_s16x2(E[k], K.neg_e2, hq);                         \
+        f = __viaddmax_s16x2(f, K.neg_e2, hq);                               \
     }
     SWB_CELL(0)
     SWB_CELL(1)
@@ -97,15 +121,15 @@ struct RowChunks {
     static __device__ __forceinline__ void run(uint32_t (&H)[R], uint32_t (&E)[R],
                                                const uint2* p0, const uint2* p1, int jstride,
                                                uint2 A, uint2 B, uint32_t& diag, uint32_t& f,
-                                               uint32_t& S, uint32_t NEG_OE, uint32_t NEG_E) {
+                                               uint32_t& S, const CellK& K) {
         uint2 An = A, Bn = B;
         if constexpr (J + 1 < NJ) {
             An = p0[(J + 1) * jstride];
             Bn = p1[(J + 1) * jstride];
         }
-        rows8<R, J>(H, E, A, B, diag, f, S, NEG_OE, NEG_E);
+        rows8<R, J>(H, E, A, B, diag, f, S, K);
         if constexpr (J + 1 < NJ)
-            RowChunks<R, J + 1, NJ>::run(H, E, p0, p1, jstride, An, Bn, diag, f, S, NEG_OE, NEG_E);
+            RowChunks<R, J + 1, NJ>::run(H, E, p0, p1, jstride, An, Bn, diag, f, S, K);
     }
 };
 
@@ -150,29 +174,47 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
     const int t = lane & (T - 1);
     const int slot = lane & (SLOTS - 1);
     const unsigned gmask = (T == 32) ? FULL : (((1u << T) - 1u) << (lane & ~(T - 1)));
-    const uint32_t NEG_OE = a.neg_oe, NEG_E = a.neg_e;
+    CellK K;
+    K.bias2 = a.bias2;
+    K.neg_q2 = 0u - a.bias2;
+    K.neg_e2 = a.neg_e;
+    K.one = a.one;
+    const uint32_t Z = a.bias2;        // biased zero of both lanes
+    const int bias = (int)(a.bias2 & 0xffffu);
 
     uint32_t H[R], E[R];
-    uint32_t S = 0;
+    uint32_t S = Z;
     int pair = 0, pass = 0, s = 0, nsteps = 0, ncols = 0, ncols_pad = 0;
     bool done = false;
     uint32_t off16 = 0;
-    uint32_t out_h = 0, out_f = 0, prev_h = 0, myd = kPadPair;
-    uint4 dbuf = make_uint4(0u, 0u, 0u, 0u);
+    uint32_t out_h = Z, out_f = Z, prev_h = Z, myd = kPadPair;
+    // thread 0 of a group: residue chunks (current, next) and the boundary row
+    // entries of the next two columns, loaded ahead so no step waits on memory
+    uint4 dcur = make_uint4(0u, 0u, 0u, 0u), dnext = dcur;
+    uint2 bq0 = make_uint2(Z, Z), bq1 = bq0;
     uint2* pbnd = a.bnd;
 
-#define SWB_START_PASS()                                \
-    {                                                   \
-        s = 0;                                          \
-        nsteps = ncols + T - 1;                         \
-        _Pragma("unroll") for (int k = 0; k < R; ++k) { \
-            H[k] = 0u;                                  \
-            E[k] = 0u;                                  \
-        }                                               \
-        out_h = 0u;                                     \
-        out_f = 0u;                                     \
-        prev_h = 0u;                                    \
-        myd = kPadPair;                                 \
+#define SWB_START_PASS()                                                  \
+    {                                                                     \
+        s = 0;                                                            \
+        nsteps = ncols + T - 1;                                           \
+        _Pragma("unroll") for (int k = 0; k < R; ++k) {                   \
+            H[k] = Z;                                                     \
+            E[k] = Z;                                                     \
+        }                                                                 \
+        out_h = Z;                                                        \
+        out_f = Z;                                                        \
+        prev_h = Z;                                                       \
+        myd = kPadPair;                                                   \
+        if (t == 0) {                                                     \
+            dcur = __ldg(a.db + off16);                                   \
+            if (ncols > 8) dnext = __ldg(a.db + off16 + 1);               \
+            if (pass > 0) {                                               \
+                const uint2* pb = pbnd + ((pass - 1) & 1) * ncols_pad;    \
+                bq0 = pb[0];                                              \
+                if (ncols > 1) bq1 = pb[1];                               \
+            }                                                             \
+        }                                                                 \
     }
 #define SWB_CLAIM()                                                      \
     {                                                                    \
@@ -191,7 +233,7 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
             ncols_pad = (ncols + 7) & ~7;                                \
             pbnd = a.bnd + (size_t)off16 * 16;                           \
             pass = 0;                                                    \
-            S = 0u;                                                      \
+            S = Z;                                                       \
             SWB_START_PASS()                                             \
         }                                                                \
     }
@@ -205,19 +247,23 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
         uint32_t f_in = __shfl_up_sync(FULL, out_f, 1, T);
         if (t == 0) {
             d_in = kPadPair;
-            h_in = 0u;
-            f_in = 0u;
+            h_in = Z;
+            f_in = Z;
             if (s < ncols) {
-                if ((s & 7) == 0) dbuf = __ldg(a.db + off16 + (s >> 3));
-                d_in = dbuf.x & 0xffffu;
-                dbuf.x = __funnelshift_r(dbuf.x, dbuf.y, 16);
-                dbuf.y = __funnelshift_r(dbuf.y, dbuf.z, 16);
-                dbuf.z = __funnelshift_r(dbuf.z, dbuf.w, 16);
-                dbuf.w >>= 16;
+                if ((s & 7) == 0 && s > 0) {
+                    dcur = dnext;
+                    if (s + 8 < ncols) dnext = __ldg(a.db + off16 + (s >> 3) + 1);
+                }
+                d_in = dcur.x & 0xffffu;
+                dcur.x = __funnelshift_r(dcur.x, dcur.y, 16);
+                dcur.y = __funnelshift_r(dcur.y, dcur.z, 16);
+                dcur.z = __funnelshift_r(dcur.z, dcur.w, 16);
+                dcur.w >>= 16;
                 if (pass > 0) {
-                    const uint2 b = pbnd[((pass - 1) & 1) * ncols_pad + s];
-                    h_in = b.x;
-                    f_in = b.y;
+                    h_in = bq0.x;
+                    f_in = bq0.y;
+                    bq0 = bq1;
+                    if (s + 2 < ncols) bq1 = pbnd[((pass - 1) & 1) * ncols_pad + s + 2];
                 }
             }
         }
@@ -227,8 +273,7 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
             const uint2* p0 = prof + ((pass * NJ) * kCodes + d0) * SLOTS + slot;
             const uint2* p1 = prof + ((pass * NJ) * kCodes + d1) * SLOTS + slot;
             uint32_t diag = prev_h, f = f_in;
-            RowChunks<R, 0, NJ>::run(H, E, p0, p1, JSTRIDE, p0[0], p1[0], diag, f, S, NEG_OE,
-                                     NEG_E);
+            RowChunks<R, 0, NJ>::run(H, E, p0, p1, JSTRIDE, p0[0], p1[0], diag, f, S, K);
             out_h = H[R - 1];
             out_f = f;
             if (t == T - 1 && pass + 1 < P) pbnd[(pass & 1) * ncols_pad + c] = make_uint2(out_h, out_f);
@@ -244,14 +289,14 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
             } else {
 #pragma unroll
                 for (int o = T / 2; o > 0; o >>= 1)
-                    S = __vimax_s16x2_relu(S, __shfl_xor_sync(gmask, S, o, T));
+                    S = __vimax3_s16x2(S, __shfl_xor_sync(gmask, S, o, T), Z);
                 if (t == 0) {
                     const int pos = 2 * (a.pair_begin + pair);
                     const int s0 = lo16(S), s1 = hi16(S);
-                    a.scores[pos] = s0;
+                    a.scores[pos] = s0 - bias;
                     if (s0 >= a.ovf_thresh) a.ovf_list[atomicAdd(a.ovf_count, 1)] = pos;
                     if (pos + 1 < a.n_records) {
-                        a.scores[pos + 1] = s1;
+                        a.scores[pos + 1] = s1 - bias;
                         if (s1 >= a.ovf_thresh) a.ovf_list[atomicAdd(a.ovf_count, 1)] = pos + 1;
                     }
                 }

@@ -71,11 +71,19 @@ def test_every_kernel_shape_bit_exact(ctx):
     res, off, queries, gold = load("homolog")
     ctx.load_db(res, off)
     try:
+        ran = 0
         for T, R in all_shapes(ctx):
             ctx.set_kernel_config((T, R, T, R, 0))
             for qi in (0, 1):
-                _, scores = ctx.search(queries[qi], want_scores=True)
+                try:
+                    _, scores = ctx.search(queries[qi], want_scores=True)
+                except capi.SwError as e:
+                    # a profile that does not fit shared memory is refused, not run
+                    assert e.status == 6, str(e)
+                    continue
+                ran += 1
                 np.testing.assert_array_equal(scores, gold[qi], err_msg=f"shape {T}x{R} q{qi}")
+        assert ran >= 80
     finally:
         ctx.set_kernel_config(None)
 
