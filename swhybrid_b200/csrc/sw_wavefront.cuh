@@ -10,15 +10,20 @@
 // at once: every H/E/F/S register holds two signed 16-bit lanes and every
 // cell update is a handful of DPX instructions.
 //
-// A group of T threads (T = 1..32, a power of two, inside one warp) owns one
-// pair.  Thread t holds R consecutive query rows in registers and walks the
-// DB columns one step behind thread t-1 (anti-diagonal wavefront): at step s
-// it updates column s - t, receiving the H/F of the row above (the last row
-// of thread t-1, one step old) and the residue pair through warp shuffles.
-// A query longer than T*R rows is done in passes; between passes the last
-// row's H/F per column goes through a double-buffered boundary row in global
-// memory.  T = 1 is the inter-sequence form (one pair per thread, boundary
-// row every R query rows); T > 1 is the warp-cooperative intra-sequence form.
+// A group of T threads (T = 1..32, a power of two, inside one warp) is a
+// systolic pipeline.  Thread t holds R consecutive query rows in registers and
+// walks DB columns one step behind thread t-1 (anti-diagonal wavefront): at
+// each step it updates one column, receiving through warp shuffles the H/F of
+// the row above (thread t-1's last row, computed one step earlier), the
+// residue pair and the column's tags.  Thread 0 feeds the pipeline with a
+// continuous stream of "segments" -- (pair, pass) column runs, one pass per
+// T*R query rows -- so the pipeline never drains between passes or pairs;
+// each thread resets its rows when the first column of a new segment reaches
+// it.  Between passes of a pair the last row's H/F per column goes through a
+// double-buffered boundary row in global memory (written by thread T-1, read
+// back two columns ahead by thread 0 of a later segment).  T = 1 is the
+// inter-sequence form (one pair per thread); T > 1 is the warp-cooperative
+// intra-sequence form.
 //
 // Recurrence per cell (same order as the reference's ONE_CELL_UPDATE,
 // src/AVXKernel.cpp:196-218, with the floor at 0 made explicit):
@@ -53,9 +58,17 @@ __host__ __device__ constexpr size_t wf_smem_bytes(int qlen) {
            GroupShape<T>::SLOTS * sizeof(uint2);
 }
 
-template <int I>
-__device__ __forceinline__ uint32_t pick_pack(const uint2& A, const uint2& B) {
-    return pack_s8x2<I & 3>(I < 4 ? A.x : A.y, I < 4 ? B.x : B.y);
+
+// Packed profile word of row I of a chunk: sign-extended int8 scores of the
+// two records' residues (low half record 2p, high half record 2p+1).
+__device__ __forceinline__ uint32_t pack_row(int i, const uint2& A, const uint2& B) {
+    const uint32_t a = i < 4 ? A.x : A.y, b = i < 4 ? B.x : B.y;
+    switch (i & 3) {
+        case 0: return pack_s8x2<0>(a, b);
+        case 1: return pack_s8x2<1>(a, b);
+        case 2: return pack_s8x2<2>(a, b);
+        default: return pack_s8x2<3>(a, b);
+    }
 }
 
 // 32-bit integer multiply-add (kept as IMAD: the multiplier is a run-time 1),
@@ -77,61 +90,54 @@ struct CellK {
     uint32_t one;       // 1, from a kernel argument
 };
 
-// One 8-row chunk of the cell recurrence (rows j*8 .. j*8+7 of this thread):
-//   t  = max(diag + P, E)            (DPX add+max)
-//   h  = max(t, F, B)                (DPX 3-way max; B = biased zero)
-//   hq = h - (open+extend)           (IMAD, both halves at once)
-//   E  = max(E - extend, hq), F = max(F - extend, hq)   (DPX add+max)
-//   S  = max(S, h, h_next)           (DPX 3-way max, every second row)
-template <int R, int J>
-__device__ __forceinline__ void rows8(uint32_t (&H)[R], uint32_t (&E)[R], const uint2 A,
-                                      const uint2 B, uint32_t& diag, uint32_t& f,
-                                      uint32_t& S, const CellK& K) {
-#define SWB_CELL(I)                                                          \
-    {                                                                        \
-        constexpr int k = J * 8 + I;                                         \
-        const uint32_t sc = pick_pack<I>(A, B);                              \
-        uint32_t h = __viaddmax_s16x2(diag, sc, E[k]);                       \
-        h = __vimax3_s16x2(h, f, K.bias2);                                   \
-        diag = H[k];                                                         \
-        H[k] = h;                                                            \
-        const uint32_t hq = mad_u32(h, K.one, K.neg_q2);                     \
-        E[k] = __viaddmax_s16x2(E[k], K.neg_e2, hq);                         \
-        f = __viaddmax_s16x2(f, K.neg_e2, hq);                               \
+// One column step over this thread's R rows.
+//   reverse:  H[k] <- max(H[k-1] + P_k, E_k)       (H[-1] = diag from above)
+//   forward:  h = max(H[k], F, B); hq = h - (open+extend);
+//             E_k = max(E_k - extend, hq); F = max(F - extend, hq); S = max(S, h)
+template <int R>
+__device__ __forceinline__ void column_step(uint32_t (&H)[R], uint32_t (&E)[R],
+                                            const uint2* p0, const uint2* p1, int jstride,
+                                            uint32_t diag, uint32_t& f, uint32_t& S,
+                                            const CellK& K) {
+    constexpr int NJ = R / 8;
+    uint2 A = p0[(NJ - 1) * jstride];
+    uint2 B = p1[(NJ - 1) * jstride];
+#pragma unroll
+    for (int j = NJ - 1; j >= 0; --j) {
+        uint2 An = A, Bn = B;
+        if (j > 0) {
+            An = p0[(j - 1) * jstride];
+            Bn = p1[(j - 1) * jstride];
+        }
+#pragma unroll
+        for (int i = 7; i >= 0; --i) {
+            const int k = j * 8 + i;
+            const uint32_t up = (k > 0) ? H[k > 0 ? k - 1 : 0] : diag;
+            H[k] = __viaddmax_s16x2(up, pack_row(i, A, B), E[k]);
+        }
+        A = An;
+        B = Bn;
     }
-    SWB_CELL(0)
-    SWB_CELL(1)
-    S = __vimax3_s16x2(S, H[J * 8 + 0], H[J * 8 + 1]);
-    SWB_CELL(2)
-    SWB_CELL(3)
-    S = __vimax3_s16x2(S, H[J * 8 + 2], H[J * 8 + 3]);
-    SWB_CELL(4)
-    SWB_CELL(5)
-    S = __vimax3_s16x2(S, H[J * 8 + 4], H[J * 8 + 5]);
-    SWB_CELL(6)
-    SWB_CELL(7)
-    S = __vimax3_s16x2(S, H[J * 8 + 6], H[J * 8 + 7]);
-#undef SWB_CELL
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const uint32_t h = __vimax3_s16x2(H[k], f, K.bias2);
+        H[k] = h;
+        const uint32_t hq = mad_u32(h, K.one, K.neg_q2);
+        E[k] = __viaddmax_s16x2(E[k], K.neg_e2, hq);
+        f = __viaddmax_s16x2(f, K.neg_e2, hq);
+        if (k & 1) S = __vimax3_s16x2(S, H[k - 1], H[k]);
+    }
 }
 
-// Chunks J..NJ-1 of one column step; the profile words of chunk J+1 are
-// loaded before chunk J is computed so the shared-memory latency overlaps.
-template <int R, int J, int NJ>
-struct RowChunks {
-    static __device__ __forceinline__ void run(uint32_t (&H)[R], uint32_t (&E)[R],
-                                               const uint2* p0, const uint2* p1, int jstride,
-                                               uint2 A, uint2 B, uint32_t& diag, uint32_t& f,
-                                               uint32_t& S, const CellK& K) {
-        uint2 An = A, Bn = B;
-        if constexpr (J + 1 < NJ) {
-            An = p0[(J + 1) * jstride];
-            Bn = p1[(J + 1) * jstride];
-        }
-        rows8<R, J>(H, E, A, B, diag, f, S, K);
-        if constexpr (J + 1 < NJ)
-            RowChunks<R, J + 1, NJ>::run(H, E, p0, p1, jstride, An, Bn, diag, f, S, K);
-    }
-};
+// Tags carried with each column word down the pipeline (low 16 bits: the
+// residue pair; bits 22..31: the pass of the column's segment).
+constexpr uint32_t kValid = 1u << 16;      // a real column
+constexpr uint32_t kFirst = 1u << 17;      // first column of a segment
+constexpr uint32_t kLast = 1u << 18;       // last column of a segment
+constexpr uint32_t kLastPass = 1u << 19;   // segment is the pair's last pass
+constexpr uint32_t kFirstPass = 1u << 20;  // segment is the pair's first pass
+constexpr uint32_t kDone = 1u << 21;       // the feeder has no more work
+constexpr int kPassShift = 22;
 
 template <int T, int R, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
@@ -173,7 +179,6 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
     const int lane = threadIdx.x & 31;
     const int t = lane & (T - 1);
     const int slot = lane & (SLOTS - 1);
-    const unsigned gmask = (T == 32) ? FULL : (((1u << T) - 1u) << (lane & ~(T - 1)));
     CellK K;
     K.bias2 = a.bias2;
     K.neg_q2 = 0u - a.bias2;
@@ -182,117 +187,147 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
     const uint32_t Z = a.bias2;        // biased zero of both lanes
     const int bias = (int)(a.bias2 & 0xffffu);
 
+    // ---- consumer state (every thread) ----
     uint32_t H[R], E[R];
-    uint32_t S = Z;
-    int pair = 0, pass = 0, s = 0, nsteps = 0, ncols = 0, ncols_pad = 0;
-    bool done = false;
-    uint32_t off16 = 0;
-    uint32_t out_h = Z, out_f = Z, prev_h = Z, myd = kPadPair;
-    // thread 0 of a group: residue chunks (current, next) and the boundary row
-    // entries of the next two columns, loaded ahead so no step waits on memory
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        H[k] = Z;
+        E[k] = Z;
+    }
+    uint32_t S = Z;                           // running max over the current pair
+    uint32_t out_h = Z, out_f = Z, out_s = Z, prev_h = Z;
+    uint32_t my_d = 0u, my_off = 0u, my_pair = 0u;
+    int col = 0;
+    bool finished = false;
+
+    // ---- feeder state (meaningful in thread 0 of each group) ----
+    int f_pair = 0, f_next = 0, f_pass = 0, f_col = 0, f_ncols = 0, f_start = -(1 << 20);
+    uint32_t f_off = 0u;
+    bool f_done = false, f_open = false;
+    Pair2 f_ninfo{0u, 0u};
     uint4 dcur = make_uint4(0u, 0u, 0u, 0u), dnext = dcur;
     uint2 bq0 = make_uint2(Z, Z), bq1 = bq0;
-    uint2* pbnd = a.bnd;
-
-#define SWB_START_PASS()                                                  \
-    {                                                                     \
-        s = 0;                                                            \
-        nsteps = ncols + T - 1;                                           \
-        _Pragma("unroll") for (int k = 0; k < R; ++k) {                   \
-            H[k] = Z;                                                     \
-            E[k] = Z;                                                     \
-        }                                                                 \
-        out_h = Z;                                                        \
-        out_f = Z;                                                        \
-        prev_h = Z;                                                       \
-        myd = kPadPair;                                                   \
-        if (t == 0) {                                                     \
-            dcur = __ldg(a.db + off16);                                   \
-            if (ncols > 8) dnext = __ldg(a.db + off16 + 1);               \
-            if (pass > 0) {                                               \
-                const uint2* pb = pbnd + ((pass - 1) & 1) * ncols_pad;    \
-                bq0 = pb[0];                                              \
-                if (ncols > 1) bq1 = pb[1];                               \
-            }                                                             \
-        }                                                                 \
-    }
-#define SWB_CLAIM()                                                      \
-    {                                                                    \
-        int v = 0;                                                       \
-        if (t == 0) v = atomicAdd(a.counter, 1);                         \
-        v = __shfl_sync(gmask, v, 0, T);                                 \
-        if (v >= a.pair_count) {                                         \
-            done = true;                                                 \
-            ncols = 0;                                                   \
-            nsteps = 0;                                                  \
-        } else {                                                         \
-            pair = v;                                                    \
-            const Pair2 pr = a.pairs[a.pair_begin + v];                  \
-            off16 = pr.off16;                                            \
-            ncols = (int)pr.ncols;                                       \
-            ncols_pad = (ncols + 7) & ~7;                                \
-            pbnd = a.bnd + (size_t)off16 * 16;                           \
-            pass = 0;                                                    \
-            S = Z;                                                       \
-            SWB_START_PASS()                                             \
-        }                                                                \
+    if (t == 0) {
+        f_pair = atomicAdd(a.counter, 1);
+        if (f_pair >= a.pair_count) {
+            f_done = true;
+        } else {
+            const Pair2 pr = a.pairs[a.pair_begin + f_pair];
+            f_off = pr.off16;
+            f_ncols = (int)pr.ncols;
+        }
     }
 
-    SWB_CLAIM()
-
-    while (!__all_sync(FULL, done)) {
-        // ---- one wavefront step: receive from the thread above ----
-        uint32_t d_in = __shfl_up_sync(FULL, myd, 1, T);
+    for (int step = 0; !__all_sync(FULL, finished); ++step) {
+        uint32_t d_in = __shfl_up_sync(FULL, my_d, 1, T);
         uint32_t h_in = __shfl_up_sync(FULL, out_h, 1, T);
         uint32_t f_in = __shfl_up_sync(FULL, out_f, 1, T);
+        uint32_t s_in = __shfl_up_sync(FULL, out_s, 1, T);
+        uint32_t o_in = __shfl_up_sync(FULL, my_off, 1, T);
+        uint32_t p_in = __shfl_up_sync(FULL, my_pair, 1, T);
+
         if (t == 0) {
-            d_in = kPadPair;
+            // ---- feeder: emit one column of the current segment ----
+            d_in = 0u;
             h_in = Z;
             f_in = Z;
-            if (s < ncols) {
-                if ((s & 7) == 0 && s > 0) {
-                    dcur = dnext;
-                    if (s + 8 < ncols) dnext = __ldg(a.db + off16 + (s >> 3) + 1);
+            s_in = Z;
+            if (f_done) {
+                d_in = kDone;
+            } else {
+                bool emit = true;
+                if (!f_open) {
+                    // open a new segment; a later pass of the same pair waits
+                    // until thread T-1 has written the boundary row ahead of it
+                    if (f_pass > 0 && step - f_start < T + 2) {
+                        emit = false;
+                    } else {
+                        f_open = true;
+                        f_col = 0;
+                        f_start = step;
+                        dcur = __ldg(a.db + f_off);
+                        if (f_ncols > 8) dnext = __ldg(a.db + f_off + 1);
+                        if (f_pass > 0) {
+                            const uint2* pb = a.bnd + (size_t)f_off * 16 + ((f_pass - 1) & 1);
+                            bq0 = pb[0];
+                            if (f_ncols > 1) bq1 = pb[2];
+                        }
+                        if (f_pass == 0) f_next = atomicAdd(a.counter, 1);
+                    }
                 }
-                d_in = dcur.x & 0xffffu;
-                dcur.x = __funnelshift_r(dcur.x, dcur.y, 16);
-                dcur.y = __funnelshift_r(dcur.y, dcur.z, 16);
-                dcur.z = __funnelshift_r(dcur.z, dcur.w, 16);
-                dcur.w >>= 16;
-                if (pass > 0) {
-                    h_in = bq0.x;
-                    f_in = bq0.y;
-                    bq0 = bq1;
-                    if (s + 2 < ncols) bq1 = pbnd[((pass - 1) & 1) * ncols_pad + s + 2];
+                if (emit) {
+                    if (f_col > 0 && (f_col & 7) == 0) {
+                        dcur = dnext;
+                        if (f_col + 8 < f_ncols) dnext = __ldg(a.db + f_off + (f_col >> 3) + 1);
+                    }
+                    uint32_t w = (dcur.x & 0xffffu) | kValid | ((uint32_t)f_pass << kPassShift);
+                    dcur.x = __funnelshift_r(dcur.x, dcur.y, 16);
+                    dcur.y = __funnelshift_r(dcur.y, dcur.z, 16);
+                    dcur.z = __funnelshift_r(dcur.z, dcur.w, 16);
+                    dcur.w >>= 16;
+                    if (f_col == 0) w |= kFirst;
+                    if (f_pass == 0) w |= kFirstPass;
+                    if (f_pass + 1 == P) w |= kLastPass;
+                    if (f_pass > 0) {
+                        h_in = bq0.x;
+                        f_in = bq0.y;
+                        bq0 = bq1;
+                        if (f_col + 2 < f_ncols)
+                            bq1 = a.bnd[(size_t)f_off * 16 + 2 * (f_col + 2) + ((f_pass - 1) & 1)];
+                    }
+                    o_in = f_off;
+                    p_in = (uint32_t)f_pair;
+                    // the next pair's table entry, once its claim has returned
+                    if (f_pass == 0 && f_col == (f_ncols < 9 ? f_ncols - 1 : 8) &&
+                        f_next < a.pair_count)
+                        f_ninfo = a.pairs[a.pair_begin + f_next];
+                    ++f_col;
+                    if (f_col == f_ncols) {
+                        w |= kLast;
+                        f_open = false;
+                        if (f_pass + 1 < P) {
+                            ++f_pass;
+                        } else if (f_next >= a.pair_count) {
+                            f_done = true;
+                        } else {
+                            f_pair = f_next;
+                            f_off = f_ninfo.off16;
+                            f_ncols = (int)f_ninfo.ncols;
+                            f_pass = 0;
+                        }
+                    }
+                    d_in = w;
                 }
             }
         }
-        const int c = s - t;
-        if (!done && c >= 0 && c < ncols) {
+
+        // ---- consumer: one column of this thread's rows ----
+        if (d_in & kValid) {
+            if (d_in & kFirst) {
+#pragma unroll
+                for (int k = 0; k < R; ++k) {
+                    H[k] = Z;
+                    E[k] = Z;
+                }
+                prev_h = Z;
+                col = 0;
+                if (d_in & kFirstPass) S = Z;
+            }
+            const int pass = (int)(d_in >> kPassShift);
             const int d0 = (int)(d_in & 0xffu), d1 = (int)((d_in >> 8) & 0xffu);
             const uint2* p0 = prof + ((pass * NJ) * kCodes + d0) * SLOTS + slot;
             const uint2* p1 = prof + ((pass * NJ) * kCodes + d1) * SLOTS + slot;
-            uint32_t diag = prev_h, f = f_in;
-            RowChunks<R, 0, NJ>::run(H, E, p0, p1, JSTRIDE, p0[0], p1[0], diag, f, S, K);
+            uint32_t f = f_in;
+            column_step<R>(H, E, p0, p1, JSTRIDE, prev_h, f, S, K);
             out_h = H[R - 1];
             out_f = f;
-            if (t == T - 1 && pass + 1 < P) pbnd[(pass & 1) * ncols_pad + c] = make_uint2(out_h, out_f);
-        }
-        prev_h = h_in;
-        myd = d_in;
-        ++s;
-        if (!done && s == nsteps) {  // uniform within the group
-            __syncwarp(gmask);
-            if (pass + 1 < P) {
-                ++pass;
-                SWB_START_PASS()
-            } else {
-#pragma unroll
-                for (int o = T / 2; o > 0; o >>= 1)
-                    S = __vimax3_s16x2(S, __shfl_xor_sync(gmask, S, o, T), Z);
-                if (t == 0) {
-                    const int pos = 2 * (a.pair_begin + pair);
-                    const int s0 = lo16(S), s1 = hi16(S);
+            if (t == T - 1 && !(d_in & kLastPass))
+                a.bnd[(size_t)o_in * 16 + 2 * col + (pass & 1)] = make_uint2(out_h, out_f);
+            if ((d_in & kLast) && (d_in & kLastPass)) {
+                out_s = __vimax3_s16x2(S, s_in, Z);
+                if (t == T - 1) {
+                    const int pos = 2 * (a.pair_begin + (int)p_in);
+                    const int s0 = lo16(out_s), s1 = hi16(out_s);
                     a.scores[pos] = s0 - bias;
                     if (s0 >= a.ovf_thresh) a.ovf_list[atomicAdd(a.ovf_count, 1)] = pos;
                     if (pos + 1 < a.n_records) {
@@ -300,12 +335,16 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
                         if (s1 >= a.ovf_thresh) a.ovf_list[atomicAdd(a.ovf_count, 1)] = pos + 1;
                     }
                 }
-                SWB_CLAIM()
             }
+            ++col;
         }
+        if (d_in & kDone) finished = true;
+        prev_h = h_in;
+        my_d = d_in;
+        my_off = o_in;
+        my_pair = p_in;
+        __syncwarp();   // orders thread T-1's boundary stores before later feeder loads
     }
-#undef SWB_CLAIM
-#undef SWB_START_PASS
 }
 
 }  // namespace swb

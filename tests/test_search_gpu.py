@@ -92,7 +92,7 @@ def test_cutover_split_bit_exact(ctx):
     res, off, queries, gold = load("homolog")
     ctx.load_db(res, off)
     try:
-        for cfg in [(32, 32, 4, 16, 400), (16, 24, 1, 32, 1000), (8, 64, 2, 40, 200)]:
+        for cfg in [(32, 32, 8, 16, 400), (16, 24, 4, 32, 1000), (8, 64, 2, 40, 200)]:
             ctx.set_kernel_config(cfg)
             for qi in (0, 1):
                 _, scores = ctx.search(queries[qi], want_scores=True)
