@@ -368,8 +368,8 @@ extern "C" sw_status sw_db_load(sw_ctx* ctx, const uint8_t* residues, const uint
     const size_t nblk = (n + kTopkKeys - 1) / kTopkKeys + 1;
     if (dev_alloc(&ctx->d_keys[0], nblk * kMaxTopK) != cudaSuccess) return nomem("keys");
     if (dev_alloc(&ctx->d_keys[1], nblk * kMaxTopK) != cudaSuccess) return nomem("keys");
-    SW_CUDA(ctx, cudaMemcpy(ctx->d_db, stream.data(), stream.size() ? stream.size() : 1,
-                            cudaMemcpyHostToDevice));
+    if (!stream.empty())
+        SW_CUDA(ctx, cudaMemcpy(ctx->d_db, stream.data(), stream.size(), cudaMemcpyHostToDevice));
     if (npairs_all)
         SW_CUDA(ctx, cudaMemcpy(ctx->d_pairs, pairs.data(), npairs_all * sizeof(Pair2),
                                 cudaMemcpyHostToDevice));

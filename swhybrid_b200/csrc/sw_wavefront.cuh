@@ -11,11 +11,13 @@
 // cell update is a handful of DPX instructions.
 //
 // A group of T threads (T = 1..32, a power of two, inside one warp) is a
-// systolic pipeline.  Thread t holds R consecutive query rows in registers and
-// walks DB columns one step behind thread t-1 (anti-diagonal wavefront): at
-// each step it updates one column, receiving through warp shuffles the H/F of
-// the row above (thread t-1's last row, computed one step earlier), the
-// residue pair and the column's tags.  Thread 0 feeds the pipeline with a
+// systolic pipeline.  Thread t holds R consecutive query rows in registers as
+// two half-columns: the top R/2 rows work on column c while the bottom R/2
+// rows work on column c-1, so every step runs two independent F chains side
+// by side (twice the instruction-level parallelism of one R-row chain).
+// Each thread receives through warp shuffles the H/F of the row above (thread
+// t-1's bottom half, one step earlier), the residue pair and the column's
+// tags, and passes its bottom half's column on to thread t+1.  Thread 0 feeds the pipeline with a
 // continuous stream of "segments" -- (pair, pass) column runs, one pass per
 // T*R query rows -- so the pipeline never drains between passes or pairs;
 // each thread resets its rows when the first column of a new segment reaches
@@ -90,43 +92,50 @@ struct CellK {
     uint32_t one;       // 1, from a kernel argument
 };
 
-// One column step over this thread's R rows.
-//   reverse:  H[k] <- max(H[k-1] + P_k, E_k)       (H[-1] = diag from above)
-//   forward:  h = max(H[k], F, B); hq = h - (open+extend);
-//             E_k = max(E_k - extend, hq); F = max(F - extend, hq); S = max(S, h)
-template <int R>
-__device__ __forceinline__ void column_step(uint32_t (&H)[R], uint32_t (&E)[R],
-                                            const uint2* p0, const uint2* p1, int jstride,
-                                            uint32_t diag, uint32_t& f, uint32_t& S,
-                                            const CellK& K) {
-    constexpr int NJ = R / 8;
-    uint2 A = p0[(NJ - 1) * jstride];
-    uint2 B = p1[(NJ - 1) * jstride];
+// Row k's profile word from a chunk pair (A: record 2p's residue, B: record
+// 2p+1's residue), sign-extended into the two 16-bit halves.
+__device__ __forceinline__ uint32_t pack_k(int k, const uint2& A, const uint2& B) {
+    return pack_row(k & 7, A, B);
+}
+
+// Reverse sweep of one half: H[k] <- max(H[k-1] + P_k, E_k) for k = HI-1 down
+// to LO, with H[LO-1] replaced by diag.  p0/p1 point at the residues' chunk 0.
+template <int R, int LO, int HI>
+__device__ __forceinline__ void reverse_sweep(uint32_t (&H)[R], const uint32_t (&E)[R],
+                                              const uint2* p0, const uint2* p1, int jstride,
+                                              uint32_t diag) {
+    constexpr int JLO = LO / 8, JHI = (HI - 1) / 8;
+    uint2 A = p0[JHI * jstride];
+    uint2 B = p1[JHI * jstride];
 #pragma unroll
-    for (int j = NJ - 1; j >= 0; --j) {
+    for (int j = JHI; j >= JLO; --j) {
         uint2 An = A, Bn = B;
-        if (j > 0) {
+        if (j > JLO) {
             An = p0[(j - 1) * jstride];
             Bn = p1[(j - 1) * jstride];
         }
 #pragma unroll
         for (int i = 7; i >= 0; --i) {
             const int k = j * 8 + i;
-            const uint32_t up = (k > 0) ? H[k > 0 ? k - 1 : 0] : diag;
-            H[k] = __viaddmax_s16x2(up, pack_row(i, A, B), E[k]);
+            if (k >= LO && k < HI) {
+                const uint32_t up = (k > LO) ? H[k > LO ? k - 1 : LO] : diag;
+                H[k] = __viaddmax_s16x2(up, pack_k(k, A, B), E[k]);
+            }
         }
         A = An;
         B = Bn;
     }
-#pragma unroll
-    for (int k = 0; k < R; ++k) {
-        const uint32_t h = __vimax3_s16x2(H[k], f, K.bias2);
-        H[k] = h;
-        const uint32_t hq = mad_u32(h, K.one, K.neg_q2);
-        E[k] = __viaddmax_s16x2(E[k], K.neg_e2, hq);
-        f = __viaddmax_s16x2(f, K.neg_e2, hq);
-        if (k & 1) S = __vimax3_s16x2(S, H[k - 1], H[k]);
-    }
+}
+
+// One forward cell: h = max(t, F, B); hq = h - (open+extend);
+// E = max(E - extend, hq); F = max(F - extend, hq).
+__device__ __forceinline__ void forward_cell(uint32_t& Hk, uint32_t& Ek, uint32_t& f,
+                                             const CellK& K) {
+    const uint32_t h = __vimax3_s16x2(Hk, f, K.bias2);
+    Hk = h;
+    const uint32_t hq = mad_u32(h, K.one, K.neg_q2);
+    Ek = __viaddmax_s16x2(Ek, K.neg_e2, hq);
+    f = __viaddmax_s16x2(f, K.neg_e2, hq);
 }
 
 // Tags carried with each column word down the pipeline (low 16 bits: the
@@ -143,6 +152,7 @@ template <int T, int R, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
     static_assert(R % 8 == 0 && R >= 8, "R");
     constexpr int NJ = R / 8;
+    constexpr int HALF = R / 2;
     constexpr int SLOTS = GroupShape<T>::SLOTS;
     constexpr int JSTRIDE = kCodes * SLOTS;
     extern __shared__ uint2 prof[];
@@ -186,18 +196,23 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
     K.one = a.one;
     const uint32_t Z = a.bias2;        // biased zero of both lanes
     const int bias = (int)(a.bias2 & 0xffffu);
+    const int pair_count = a.pair_count;
 
-    // ---- consumer state (every thread) ----
+    // ---- pipeline state (every thread) ----
+    // rows [0, HALF): top half, on the column of d_top; rows [HALF, R): bottom
+    // half, one column behind, on the column of d_bot.
     uint32_t H[R], E[R];
 #pragma unroll
     for (int k = 0; k < R; ++k) {
         H[k] = Z;
         E[k] = Z;
     }
-    uint32_t S = Z;                           // running max over the current pair
+    uint32_t S_top = Z, S_bot = Z, S_topfin = Z;
     uint32_t out_h = Z, out_f = Z, out_s = Z, prev_h = Z;
-    uint32_t my_d = 0u, my_off = 0u, my_pair = 0u;
-    int col = 0;
+    uint32_t mid_h = Z, mid_f = Z;     // top's last row: H one column back, F out
+    uint32_t d_bot = 0u, o_bot = 0u, p_bot = 0u;   // the bottom half's next column
+    uint32_t d_out = 0u, o_out = 0u, p_out = 0u;   // the column it just processed
+    int col_bot = 0;
     bool finished = false;
 
     // ---- feeder state (meaningful in thread 0 of each group) ----
@@ -209,7 +224,7 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
     uint2 bq0 = make_uint2(Z, Z), bq1 = bq0;
     if (t == 0) {
         f_pair = atomicAdd(a.counter, 1);
-        if (f_pair >= a.pair_count) {
+        if (f_pair >= pair_count) {
             f_done = true;
         } else {
             const Pair2 pr = a.pairs[a.pair_begin + f_pair];
@@ -219,12 +234,14 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
     }
 
     for (int step = 0; !__all_sync(FULL, finished); ++step) {
-        uint32_t d_in = __shfl_up_sync(FULL, my_d, 1, T);
+        // what the thread above handed down: the column its bottom half
+        // processed in the previous step, with that column's outputs
+        uint32_t d_in = __shfl_up_sync(FULL, d_out, 1, T);
         uint32_t h_in = __shfl_up_sync(FULL, out_h, 1, T);
         uint32_t f_in = __shfl_up_sync(FULL, out_f, 1, T);
         uint32_t s_in = __shfl_up_sync(FULL, out_s, 1, T);
-        uint32_t o_in = __shfl_up_sync(FULL, my_off, 1, T);
-        uint32_t p_in = __shfl_up_sync(FULL, my_pair, 1, T);
+        uint32_t o_in = __shfl_up_sync(FULL, o_out, 1, T);
+        uint32_t p_in = __shfl_up_sync(FULL, p_out, 1, T);
 
         if (t == 0) {
             // ---- feeder: emit one column of the current segment ----
@@ -239,7 +256,7 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
                 if (!f_open) {
                     // open a new segment; a later pass of the same pair waits
                     // until thread T-1 has written the boundary row ahead of it
-                    if (f_pass > 0 && step - f_start < T + 2) {
+                    if (f_pass > 0 && step - f_start < 2 * T + 2) {
                         emit = false;
                     } else {
                         f_open = true;
@@ -279,7 +296,7 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
                     p_in = (uint32_t)f_pair;
                     // the next pair's table entry, once its claim has returned
                     if (f_pass == 0 && f_col == (f_ncols < 9 ? f_ncols - 1 : 8) &&
-                        f_next < a.pair_count)
+                        f_next < pair_count)
                         f_ninfo = a.pairs[a.pair_begin + f_next];
                     ++f_col;
                     if (f_col == f_ncols) {
@@ -287,7 +304,7 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
                         f_open = false;
                         if (f_pass + 1 < P) {
                             ++f_pass;
-                        } else if (f_next >= a.pair_count) {
+                        } else if (f_next >= pair_count) {
                             f_done = true;
                         } else {
                             f_pair = f_next;
@@ -301,32 +318,72 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
             }
         }
 
-        // ---- consumer: one column of this thread's rows ----
-        if (d_in & kValid) {
-            if (d_in & kFirst) {
+        const uint32_t d_top = d_in;
+        const bool top_valid = (d_top & kValid) != 0, bot_valid = (d_bot & kValid) != 0;
+        const bool top_first = (d_top & kFirst) != 0, bot_first = (d_bot & kFirst) != 0;
+        // resets at a segment's first column (warp-uniform branch, rare)
+        if (__any_sync(FULL, top_first || bot_first)) {
 #pragma unroll
-                for (int k = 0; k < R; ++k) {
-                    H[k] = Z;
-                    E[k] = Z;
-                }
-                prev_h = Z;
-                col = 0;
-                if (d_in & kFirstPass) S = Z;
+            for (int k = 0; k < HALF; ++k) {
+                H[k] = top_first ? Z : H[k];
+                E[k] = top_first ? Z : E[k];
             }
-            const int pass = (int)(d_in >> kPassShift);
-            const int d0 = (int)(d_in & 0xffu), d1 = (int)((d_in >> 8) & 0xffu);
-            const uint2* p0 = prof + ((pass * NJ) * kCodes + d0) * SLOTS + slot;
-            const uint2* p1 = prof + ((pass * NJ) * kCodes + d1) * SLOTS + slot;
-            uint32_t f = f_in;
-            column_step<R>(H, E, p0, p1, JSTRIDE, prev_h, f, S, K);
+#pragma unroll
+            for (int k = HALF; k < R; ++k) {
+                H[k] = bot_first ? Z : H[k];
+                E[k] = bot_first ? Z : E[k];
+            }
+            if (top_first) prev_h = Z;
+            if (bot_first) {
+                mid_h = Z;
+                col_bot = 0;
+            }
+            if (top_first && (d_top & kFirstPass)) S_top = Z;
+            if (bot_first && (d_bot & kFirstPass)) S_bot = Z;
+        }
+        const uint32_t bot_diag = mid_h, bot_f_in = mid_f, topfin = S_topfin;
+        uint32_t f_top = f_in, f_bot = bot_f_in;
+        if (top_valid | bot_valid) {
+            // a half without a real column runs on zero-score residues: like a
+            // trailing padding column it cannot raise any score, and its rows
+            // are reset before they are used again
+            const uint32_t wt = top_valid ? d_top : kPadPair;
+            const uint32_t wb = bot_valid ? d_bot : kPadPair;
+            const int pt = (int)(wt >> kPassShift), pb = (int)(wb >> kPassShift);
+            const uint2* t0 = prof + ((pt * NJ) * kCodes + (int)(wt & 0xffu)) * SLOTS + slot;
+            const uint2* t1 = prof + ((pt * NJ) * kCodes + (int)((wt >> 8) & 0xffu)) * SLOTS + slot;
+            const uint2* b0 = prof + ((pb * NJ) * kCodes + (int)(wb & 0xffu)) * SLOTS + slot;
+            const uint2* b1 = prof + ((pb * NJ) * kCodes + (int)((wb >> 8) & 0xffu)) * SLOTS + slot;
+            // the top's last row before this column: the bottom's diagonal next step
+            mid_h = H[HALF - 1];
+            reverse_sweep<R, 0, HALF>(H, E, t0, t1, JSTRIDE, prev_h);
+            reverse_sweep<R, HALF, R>(H, E, b0, b1, JSTRIDE, bot_diag);
+#pragma unroll
+            for (int i = 0; i < HALF; ++i) {
+                forward_cell(H[i], E[i], f_top, K);
+                forward_cell(H[HALF + i], E[HALF + i], f_bot, K);
+                if (i & 1) {
+                    S_top = __vimax3_s16x2(S_top, H[i - 1], H[i]);
+                    S_bot = __vimax3_s16x2(S_bot, H[HALF + i - 1], H[HALF + i]);
+                } else if (i == HALF - 1) {
+                    S_top = __vimax3_s16x2(S_top, H[i], Z);
+                    S_bot = __vimax3_s16x2(S_bot, H[HALF + i], Z);
+                }
+            }
+        }
+        mid_f = f_top;
+        if (top_valid && (d_top & kLast) && (d_top & kLastPass))
+            S_topfin = __vimax3_s16x2(S_top, s_in, Z);
+        if (bot_valid) {
             out_h = H[R - 1];
-            out_f = f;
-            if (t == T - 1 && !(d_in & kLastPass))
-                a.bnd[(size_t)o_in * 16 + 2 * col + (pass & 1)] = make_uint2(out_h, out_f);
-            if ((d_in & kLast) && (d_in & kLastPass)) {
-                out_s = __vimax3_s16x2(S, s_in, Z);
+            out_f = f_bot;
+            const int pb = (int)(d_bot >> kPassShift);
+            if (t == T - 1 && !(d_bot & kLastPass))
+                a.bnd[(size_t)o_bot * 16 + 2 * col_bot + (pb & 1)] = make_uint2(out_h, out_f);
+            if ((d_bot & kLast) && (d_bot & kLastPass)) {
+                out_s = __vimax3_s16x2(S_bot, topfin, Z);
                 if (t == T - 1) {
-                    const int pos = 2 * (a.pair_begin + (int)p_in);
+                    const int pos = 2 * (a.pair_begin + (int)p_bot);
                     const int s0 = lo16(out_s), s1 = hi16(out_s);
                     a.scores[pos] = s0 - bias;
                     if (s0 >= a.ovf_thresh) a.ovf_list[atomicAdd(a.ovf_count, 1)] = pos;
@@ -336,13 +393,16 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
                     }
                 }
             }
-            ++col;
+            ++col_bot;
         }
-        if (d_in & kDone) finished = true;
+        if (d_bot & kDone) finished = true;
         prev_h = h_in;
-        my_d = d_in;
-        my_off = o_in;
-        my_pair = p_in;
+        d_out = d_bot;
+        o_out = o_bot;
+        p_out = p_bot;
+        d_bot = d_top;
+        o_bot = o_in;
+        p_bot = p_in;
         __syncwarp();   // orders thread T-1's boundary stores before later feeder loads
     }
 }

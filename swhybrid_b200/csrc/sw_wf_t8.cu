@@ -11,7 +11,7 @@ constexpr WfKernel inst() {
 }  // namespace
 
 extern const WfKernel wf_table_t8[] = {
-    inst<8, 768>(),  inst<16, 768>(), inst<24, 512>(), inst<32, 384>(),
+    inst<8, 768>(),  inst<16, 640>(), inst<24, 512>(), inst<32, 384>(),
     inst<40, 384>(), inst<48, 256>(), inst<56, 256>(), inst<64, 256>(),
 };
 extern const int wf_table_t8_n = sizeof(wf_table_t8) / sizeof(wf_table_t8[0]);
