@@ -173,6 +173,9 @@ def probe_rates(device: int):
         "lop3_instr_per_clk_sm": per(out[7], 1),
         "cell_mix_v1_gcups": out[3] / 1e9,
         "cell_mix_gcups": out[8] / 1e9,
+        "hmax2_instr_per_clk_sm": per(out[11], 2),
+        "hadd2_instr_per_clk_sm": per(out[12], 2),
+        "hmax2_dpx_mix_instr_per_clk_sm": per(out[13], 2),
         "sms": int(sms), "attr_clock_mhz": mhz,
     }
 

@@ -44,7 +44,8 @@ def time_shape(ctx: capi.Context, dq, qlen: int, cfg: tuple, reps: int = 2) -> f
     return t.cells / (t.first_pass_ms * 1e-3) / 1e9
 
 
-def sweep(ctx: capi.Context, lengths, shapes=None, reps: int = 2, log=print):
+def sweep(ctx: capi.Context, lengths, shapes=None, reps: int = 2, log=print,
+          cutovers=(2048, 4096, 8192, 16384)):
     import torch
     shapes = shapes or [(T, R) for T in GROUP_WIDTHS for R in ROWS]
     results = {}
@@ -57,8 +58,19 @@ def sweep(ctx: capi.Context, lengths, shapes=None, reps: int = 2, log=print):
             if g is not None:
                 row[f"{T}x{R}"] = round(g, 1)
         best = max(row, key=row.get)
-        results[int(L)] = {"best": best, "gcups": row[best], "all": row}
-        log(f"qlen {L}: best {best} {row[best]:.0f} GCUPS")
+        T, R = (int(x) for x in best.split("x"))
+        cut = {}
+        for c in cutovers:
+            g = time_shape(ctx, dq, int(L), (T, R, T, R, c), reps)
+            if g is not None:
+                cut[c] = round(g, 1)
+        best_cut = max(cut, key=cut.get) if cut else 0
+        if cut and cut[best_cut] <= row[best]:
+            best_cut = 0
+        results[int(L)] = {"best": best, "cutover": int(best_cut),
+                           "gcups": max(row[best], cut.get(best_cut, 0.0)),
+                           "all": row, "cutovers": {str(k): v for k, v in cut.items()}}
+        log(f"qlen {L}: best {best} cut-over {best_cut} {results[int(L)]['gcups']:.0f} GCUPS")
     ctx.set_kernel_config(None)
     return results
 
@@ -71,7 +83,7 @@ def table_from_sweep(results) -> list:
     for i, L in enumerate(Ls):
         hi = int(np.sqrt(L * Ls[i + 1])) if i + 1 < len(Ls) else 1 << 30
         T, R = (int(x) for x in results[L]["best"].split("x"))
-        out.append((hi, (T, R, T, R, 0)))
+        out.append((hi, (T, R, T, R, int(results[L].get("cutover", 0)))))
     return out
 
 
@@ -102,15 +114,19 @@ def apply(ctx: capi.Context, path: str = DEFAULT_TABLE) -> bool:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=DEFAULT_TABLE)
-    ap.add_argument("--records", type=int, default=142_500)
-    ap.add_argument("--long", type=int, default=50)
-    ap.add_argument("--reps", type=int, default=2)
+    ap.add_argument("--records", type=int, default=570_000)
+    ap.add_argument("--long", type=int, default=200)
+    ap.add_argument("--reps", type=int, default=1)
+    ap.add_argument("--widths", type=str, default="8,16,32",
+                    help="group widths to try (comma separated)")
     args = ap.parse_args()
+    widths = [int(x) for x in args.widths.split(",")]
     db = synth.full_db(7, args.records, args.long)
     ctx = capi.Context(0)
     ctx.load_db(db.residues, db.offsets)
     t0 = time.time()
-    res = sweep(ctx, synth.sweep_lengths(), reps=args.reps)
+    res = sweep(ctx, synth.sweep_lengths(), shapes=[(T, R) for T in widths for R in ROWS],
+                reps=args.reps)
     import torch
     save(res, args.out, meta={"gpu": torch.cuda.get_device_name(0), "records": db.n,
                               "residues": db.total, "seconds": round(time.time() - t0, 1)})

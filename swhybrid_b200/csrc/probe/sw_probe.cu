@@ -16,10 +16,13 @@
 //   op 8  the first pass's per-row cell recurrence as sw_wavefront.cuh runs
 //         it (4 DPX + 1 IMAD + 1 PRMT per row, 1 three-way max per two rows),
 //         without its shared-memory loads and shuffles
+//   op 9  __hmax2 (half2 max), op 10 __hadd2, op 11 __hmax2 and
+//         __viaddmax_s16x2 interleaved 1:1 (does half2 max use another pipe?)
 // Rates are returned in lane-operations per second (ops 0-2, 4-7; a 16x2
 // operation counts as two) and in cell updates per second (ops 3 and 8, two
 // cells per row and register).
 #include <cstdint>
+#include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 namespace {
@@ -57,6 +60,13 @@ __global__ void __launch_bounds__(512) rate_kernel(uint32_t* sink, int iters, ui
                 a[j] = r;
             }
             if (OP == 7) a[j] = (a[j] & a[j ^ 1]) ^ b;
+            if (OP == 9 || OP == 10 || (OP == 11 && (j & 1))) {
+                __half2 x = *reinterpret_cast<__half2*>(&a[j]);
+                __half2 y = *reinterpret_cast<__half2*>(&a[j ^ 1]);
+                __half2 r = (OP == 10) ? __hadd2(x, y) : __hmax2(x, y);
+                a[j] = *reinterpret_cast<uint32_t*>(&r);
+            }
+            if (OP == 11 && !(j & 1)) a[j] = __viaddmax_s16x2(a[j], b, a[j ^ 1]);
         }
         b += c;
     }
@@ -171,8 +181,8 @@ double time_kernel(K kern, int sms, int iters, uint32_t* sink, double work_per_t
 }  // namespace
 
 // out[0..8] = rates of ops 0..8 (see the file comment); out[9] = SM count;
-// out[10] = SM clock in MHz reported by the device attribute.  Returns 0 on
-// success.
+// out[10] = SM clock in MHz reported by the device attribute; out[11..13] =
+// rates of ops 9..11.  Returns 0 on success.
 extern "C" int swprobe_rates(int device, double* out, int iters) {
     if (cudaSetDevice(device) != cudaSuccess) return 1;
     int sms = 0, clk = 0;
@@ -192,6 +202,9 @@ extern "C" int swprobe_rates(int device, double* out, int iters) {
     out[8] = time_kernel(cell2_kernel, sms, iters / 4, sink, 16.0 * 2);
     out[9] = sms;
     out[10] = clk / 1000.0;
+    out[11] = time_kernel(rate_kernel<9>, sms, iters, sink, 16.0);
+    out[12] = time_kernel(rate_kernel<10>, sms, iters, sink, 16.0);
+    out[13] = time_kernel(rate_kernel<11>, sms, iters, sink, 16.0);
     cudaFree(sink);
     return cudaGetLastError() == cudaSuccess ? 0 : 3;
 }

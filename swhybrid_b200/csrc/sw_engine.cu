@@ -222,6 +222,10 @@ extern "C" sw_status sw_ctx_create(int device, const sw_params* params, sw_ctx**
     if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess)
         return fail(SW_ERR_CUDA);
     ctx->stream = ctx->own_stream;
+    if (cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming) != cudaSuccess)
+        return fail(SW_ERR_CUDA);
     for (auto& e : ctx->ev)
         if (cudaEventCreate(&e) != cudaSuccess) return fail(SW_ERR_CUDA);
     // matrix: int8 copy; codes >= 24 (zero code, pads) score 0
@@ -270,6 +274,7 @@ extern "C" sw_status sw_ctx_destroy(sw_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
+    if (ctx->side_stream) cudaStreamSynchronize(ctx->side_stream);
     free_db(ctx);
     dev_free(ctx->d_mat);
     dev_free(ctx->d_counters);
@@ -281,6 +286,9 @@ extern "C" sw_status sw_ctx_destroy(sw_ctx* ctx) {
     for (auto* v : {&ctx->pending, &ctx->spare})
         for (auto& m : *v)
             for (auto& e : m.e) cudaEventDestroy(e);
+    if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+    if (ctx->join_ev) cudaEventDestroy(ctx->join_ev);
+    if (ctx->side_stream) cudaStreamDestroy(ctx->side_stream);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return SW_OK;
@@ -541,7 +549,18 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
     } segs[2] = {{cfg.long_group_width, cfg.long_rows_per_thread, 0, n_long, 0},
                  {cfg.short_group_width, cfg.short_rows_per_thread, n_long, ctx->n_pairs, 1}};
     const int ovf_thresh = 32767 - std::max(ctx->max_score, 1) + 1;
-    for (const Seg& sg : segs) {
+    // With a cut-over, the long pairs run concurrently on the side stream in
+    // blocks of 128 threads that request the whole shared memory of an SM:
+    // each such SM then holds one of them and nothing else, so the few long
+    // pairs (whose steps are inherently serial) get a warp scheduler each
+    // instead of queueing behind the bulk; the bulk takes the other SMs.
+    const bool split = cfg.cutover > 0 && n_long > 0 && n_long < ctx->n_pairs;
+    if (split) {
+        SW_CUDA(ctx, cudaEventRecord(ctx->fork_ev, st));
+        SW_CUDA(ctx, cudaStreamWaitEvent(ctx->side_stream, ctx->fork_ev, 0));
+    }
+    for (int si = 0; si < 2; ++si) {
+        const Seg& sg = segs[si];
         if (sg.e <= sg.b) continue;
         const WfKernel* k = find_kernel(sg.T, sg.R);
         if (!k) SW_SET(ctx, SW_ERR_INVALID, "no kernel %dx%d", sg.T, sg.R);
@@ -571,15 +590,28 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
         a.ovf_count = ctx->d_counters + 2;
         a.ovf_thresh = ovf_thresh;
         const int64_t groups_needed = (sg.e - sg.b);
-        int64_t grid = (int64_t)occ * ctx->num_sms;
-        const int64_t groups_per_block = k->block / k->T;
-        grid = std::min<int64_t>(grid, (groups_needed + groups_per_block - 1) / groups_per_block);
-        grid = std::max<int64_t>(grid, 1);
         void* args[] = {&a};
-        SW_CUDA(ctx, cudaLaunchKernel(k->fn, dim3((unsigned)grid), dim3(k->block), args,
-                                      k->smem(qlen), st));
+        if (split && si == 0) {
+            const int threads = std::max(128, k->T);
+            const int64_t gpb = threads / k->T;
+            int64_t grid = (groups_needed + gpb - 1) / gpb;
+            grid = std::max<int64_t>(1, std::min<int64_t>(grid, ctx->num_sms / 2));
+            SW_CUDA(ctx, cudaLaunchKernel(k->fn, dim3((unsigned)grid), dim3(threads), args,
+                                          (size_t)ctx->max_smem, ctx->side_stream));
+        } else {
+            int64_t grid = (int64_t)occ * ctx->num_sms;
+            const int64_t groups_per_block = k->block / k->T;
+            grid = std::min<int64_t>(grid, (groups_needed + groups_per_block - 1) / groups_per_block);
+            grid = std::max<int64_t>(grid, 1);
+            SW_CUDA(ctx, cudaLaunchKernel(k->fn, dim3((unsigned)grid), dim3(k->block), args,
+                                          k->smem(qlen), st));
+        }
         ++*launches;
         ++mk.fp_launches;
+    }
+    if (split) {
+        SW_CUDA(ctx, cudaEventRecord(ctx->join_ev, ctx->side_stream));
+        SW_CUDA(ctx, cudaStreamWaitEvent(st, ctx->join_ev, 0));
     }
     SW_CUDA(ctx, cudaEventRecord(mk.e[2], st));
     {

@@ -15,6 +15,8 @@ struct sw_ctx {
     int max_smem = 0;
     cudaStream_t stream = nullptr;       // stream in use
     cudaStream_t own_stream = nullptr;   // the context's own stream
+    cudaStream_t side_stream = nullptr;  // concurrent launch of the long-record pairs
+    cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     // timing events of enqueued searches: begin, first pass begin/end, end
     struct Marks {

@@ -10,22 +10,19 @@
 // at once: every H/E/F/S register holds two signed 16-bit lanes and every
 // cell update is a handful of DPX instructions.
 //
-// A group of T threads (T = 1..32, a power of two, inside one warp) is a
-// systolic pipeline.  Thread t holds R consecutive query rows in registers as
-// two half-columns: the top R/2 rows work on column c while the bottom R/2
-// rows work on column c-1, so every step runs two independent F chains side
-// by side (twice the instruction-level parallelism of one R-row chain).
-// Each thread receives through warp shuffles the H/F of the row above (thread
-// t-1's bottom half, one step earlier), the residue pair and the column's
-// tags, and passes its bottom half's column on to thread t+1.  Thread 0 feeds the pipeline with a
-// continuous stream of "segments" -- (pair, pass) column runs, one pass per
-// T*R query rows -- so the pipeline never drains between passes or pairs;
-// each thread resets its rows when the first column of a new segment reaches
-// it.  Between passes of a pair the last row's H/F per column goes through a
-// double-buffered boundary row in global memory (written by thread T-1, read
-// back two columns ahead by thread 0 of a later segment).  T = 1 is the
-// inter-sequence form (one pair per thread); T > 1 is the warp-cooperative
-// intra-sequence form.
+// A group of T threads (T = 1..32, a power of two, inside one warp) owns one
+// pair at a time.  Thread t holds R consecutive query rows in registers as two
+// half-columns: the top R/2 rows work on column c while the bottom R/2 rows
+// work on column c-1, so every step runs two independent F chains side by side
+// (twice the instruction-level parallelism of one R-row chain).  Thread t's
+// top half trails thread t-1's bottom half by one step (anti-diagonal
+// wavefront): through warp shuffles it receives the H/F of the row above and
+// the residue pair.  Thread 0 streams the pair's columns (prefetched 16-byte
+// chunks).  A query longer than T*R rows is done in passes; between passes
+// the last row's H/F per column goes through a double-buffered boundary row
+// in global memory (written by thread T-1, read back two columns ahead by
+// thread 0).  T = 1 is the inter-sequence form (one pair per thread); T > 1
+// is the warp-cooperative intra-sequence form.
 //
 // Recurrence per cell (same order as the reference's ONE_CELL_UPDATE,
 // src/AVXKernel.cpp:196-218, with the floor at 0 made explicit):
@@ -138,16 +135,6 @@ __device__ __forceinline__ void forward_cell(uint32_t& Hk, uint32_t& Ek, uint32_
     f = __viaddmax_s16x2(f, K.neg_e2, hq);
 }
 
-// Tags carried with each column word down the pipeline (low 16 bits: the
-// residue pair; bits 22..31: the pass of the column's segment).
-constexpr uint32_t kValid = 1u << 16;      // a real column
-constexpr uint32_t kFirst = 1u << 17;      // first column of a segment
-constexpr uint32_t kLast = 1u << 18;       // last column of a segment
-constexpr uint32_t kLastPass = 1u << 19;   // segment is the pair's last pass
-constexpr uint32_t kFirstPass = 1u << 20;  // segment is the pair's first pass
-constexpr uint32_t kDone = 1u << 21;       // the feeder has no more work
-constexpr int kPassShift = 22;
-
 template <int T, int R, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
     static_assert(R % 8 == 0 && R >= 8, "R");
@@ -163,7 +150,7 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
     // ---- query profile -> shared memory (once per block) ----
     {
         const int total = P * NJ * JSTRIDE;
-        for (int idx = threadIdx.x; idx < total; idx += BLOCK) {
+        for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
             const int slot = idx % SLOTS;
             int rest = idx / SLOTS;
             const int d = rest % kCodes;
@@ -189,6 +176,7 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
     const int lane = threadIdx.x & 31;
     const int t = lane & (T - 1);
     const int slot = lane & (SLOTS - 1);
+    const unsigned gmask = (T == 32) ? FULL : (((1u << T) - 1u) << (lane & ~(T - 1)));
     CellK K;
     K.bias2 = a.bias2;
     K.neg_q2 = 0u - a.bias2;
@@ -198,193 +186,155 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
     const int bias = (int)(a.bias2 & 0xffffu);
     const int pair_count = a.pair_count;
 
-    // ---- pipeline state (every thread) ----
-    // rows [0, HALF): top half, on the column of d_top; rows [HALF, R): bottom
-    // half, one column behind, on the column of d_bot.
+    // rows [0, HALF): top half, on column s - 2t; rows [HALF, R): bottom half,
+    // on column s - 2t - 1 (s = step within the pass)
     uint32_t H[R], E[R];
-#pragma unroll
-    for (int k = 0; k < R; ++k) {
-        H[k] = Z;
-        E[k] = Z;
-    }
-    uint32_t S_top = Z, S_bot = Z, S_topfin = Z;
-    uint32_t out_h = Z, out_f = Z, out_s = Z, prev_h = Z;
-    uint32_t mid_h = Z, mid_f = Z;     // top's last row: H one column back, F out
-    uint32_t d_bot = 0u, o_bot = 0u, p_bot = 0u;   // the bottom half's next column
-    uint32_t d_out = 0u, o_out = 0u, p_out = 0u;   // the column it just processed
-    int col_bot = 0;
-    bool finished = false;
-
-    // ---- feeder state (meaningful in thread 0 of each group) ----
-    int f_pair = 0, f_next = 0, f_pass = 0, f_col = 0, f_ncols = 0, f_start = -(1 << 20);
-    uint32_t f_off = 0u;
-    bool f_done = false, f_open = false;
-    Pair2 f_ninfo{0u, 0u};
+    uint32_t S = Z;
+    uint32_t out_h = Z, out_f = Z, prev_h = Z, mid_h = Z, mid_f = Z;
+    uint32_t d_bot = kPadPair, d_out = kPadPair;
+    int pair = 0, next = 0, pass = 0, s = 0, nsteps = 0, ncols = 0;
+    uint32_t off16 = 0u;
+    bool done = false;
+    // thread 0 of a group: residue chunks (current, next), boundary entries of
+    // the next two columns, and the next pair (claimed one pair ahead)
     uint4 dcur = make_uint4(0u, 0u, 0u, 0u), dnext = dcur;
     uint2 bq0 = make_uint2(Z, Z), bq1 = bq0;
-    if (t == 0) {
-        f_pair = atomicAdd(a.counter, 1);
-        if (f_pair >= pair_count) {
-            f_done = true;
-        } else {
-            const Pair2 pr = a.pairs[a.pair_begin + f_pair];
-            f_off = pr.off16;
-            f_ncols = (int)pr.ncols;
-        }
+    Pair2 ninfo{0u, 0u};
+
+#define SWB_START_PASS()                                                   \
+    {                                                                      \
+        s = 0;                                                             \
+        nsteps = ncols + 2 * T - 1;                                        \
+        _Pragma("unroll") for (int k = 0; k < R; ++k) {                    \
+            H[k] = Z;                                                      \
+            E[k] = Z;                                                      \
+        }                                                                  \
+        out_h = Z;                                                         \
+        out_f = Z;                                                         \
+        prev_h = Z;                                                        \
+        mid_h = Z;                                                         \
+        mid_f = Z;                                                         \
+        d_bot = kPadPair;                                                  \
+        d_out = kPadPair;                                                  \
+        if (t == 0) {                                                      \
+            dcur = __ldg(a.db + off16);                                    \
+            if (ncols > 8) dnext = __ldg(a.db + off16 + 1);                \
+            if (pass > 0) {                                                \
+                const uint2* pb = a.bnd + (size_t)off16 * 16 + ((pass - 1) & 1); \
+                bq0 = pb[0];                                               \
+                if (ncols > 1) bq1 = pb[2];                                \
+            }                                                              \
+        }                                                                  \
+    }
+#define SWB_TAKE_PAIR(v)                                                   \
+    {                                                                      \
+        if ((v) >= pair_count) {                                           \
+            done = true;                                                   \
+            ncols = 0;                                                     \
+            nsteps = 0;                                                    \
+        } else {                                                           \
+            pair = (v);                                                    \
+            pass = 0;                                                      \
+            S = Z;                                                         \
+            if (t == 0) next = atomicAdd(a.counter, 1);                    \
+            SWB_START_PASS()                                               \
+        }                                                                  \
     }
 
-    for (int step = 0; !__all_sync(FULL, finished); ++step) {
-        // what the thread above handed down: the column its bottom half
-        // processed in the previous step, with that column's outputs
+    {
+        int v = 0;
+        if (t == 0) v = atomicAdd(a.counter, 1);
+        v = __shfl_sync(gmask, v, 0, T);
+        if (v < pair_count) {
+            const Pair2 pr = a.pairs[a.pair_begin + v];
+            off16 = pr.off16;
+            ncols = (int)pr.ncols;
+        }
+        SWB_TAKE_PAIR(v)
+    }
+
+    while (!__all_sync(FULL, done)) {
+        // thread t-1's bottom half handed down the column it processed in the
+        // previous step, with that column's last-row H and F
         uint32_t d_in = __shfl_up_sync(FULL, d_out, 1, T);
         uint32_t h_in = __shfl_up_sync(FULL, out_h, 1, T);
         uint32_t f_in = __shfl_up_sync(FULL, out_f, 1, T);
-        uint32_t s_in = __shfl_up_sync(FULL, out_s, 1, T);
-        uint32_t o_in = __shfl_up_sync(FULL, o_out, 1, T);
-        uint32_t p_in = __shfl_up_sync(FULL, p_out, 1, T);
-
         if (t == 0) {
-            // ---- feeder: emit one column of the current segment ----
-            d_in = 0u;
+            d_in = kPadPair;
             h_in = Z;
             f_in = Z;
-            s_in = Z;
-            if (f_done) {
-                d_in = kDone;
-            } else {
-                bool emit = true;
-                if (!f_open) {
-                    // open a new segment; a later pass of the same pair waits
-                    // until thread T-1 has written the boundary row ahead of it
-                    if (f_pass > 0 && step - f_start < 2 * T + 2) {
-                        emit = false;
-                    } else {
-                        f_open = true;
-                        f_col = 0;
-                        f_start = step;
-                        dcur = __ldg(a.db + f_off);
-                        if (f_ncols > 8) dnext = __ldg(a.db + f_off + 1);
-                        if (f_pass > 0) {
-                            const uint2* pb = a.bnd + (size_t)f_off * 16 + ((f_pass - 1) & 1);
-                            bq0 = pb[0];
-                            if (f_ncols > 1) bq1 = pb[2];
-                        }
-                        if (f_pass == 0) f_next = atomicAdd(a.counter, 1);
-                    }
+            if (s < ncols) {
+                if (s > 0 && (s & 7) == 0) {
+                    dcur = dnext;
+                    if (s + 8 < ncols) dnext = __ldg(a.db + off16 + (s >> 3) + 1);
                 }
-                if (emit) {
-                    if (f_col > 0 && (f_col & 7) == 0) {
-                        dcur = dnext;
-                        if (f_col + 8 < f_ncols) dnext = __ldg(a.db + f_off + (f_col >> 3) + 1);
-                    }
-                    uint32_t w = (dcur.x & 0xffffu) | kValid | ((uint32_t)f_pass << kPassShift);
-                    dcur.x = __funnelshift_r(dcur.x, dcur.y, 16);
-                    dcur.y = __funnelshift_r(dcur.y, dcur.z, 16);
-                    dcur.z = __funnelshift_r(dcur.z, dcur.w, 16);
-                    dcur.w >>= 16;
-                    if (f_col == 0) w |= kFirst;
-                    if (f_pass == 0) w |= kFirstPass;
-                    if (f_pass + 1 == P) w |= kLastPass;
-                    if (f_pass > 0) {
-                        h_in = bq0.x;
-                        f_in = bq0.y;
-                        bq0 = bq1;
-                        if (f_col + 2 < f_ncols)
-                            bq1 = a.bnd[(size_t)f_off * 16 + 2 * (f_col + 2) + ((f_pass - 1) & 1)];
-                    }
-                    o_in = f_off;
-                    p_in = (uint32_t)f_pair;
-                    // the next pair's table entry, once its claim has returned
-                    if (f_pass == 0 && f_col == (f_ncols < 9 ? f_ncols - 1 : 8) &&
-                        f_next < pair_count)
-                        f_ninfo = a.pairs[a.pair_begin + f_next];
-                    ++f_col;
-                    if (f_col == f_ncols) {
-                        w |= kLast;
-                        f_open = false;
-                        if (f_pass + 1 < P) {
-                            ++f_pass;
-                        } else if (f_next >= pair_count) {
-                            f_done = true;
-                        } else {
-                            f_pair = f_next;
-                            f_off = f_ninfo.off16;
-                            f_ncols = (int)f_ninfo.ncols;
-                            f_pass = 0;
-                        }
-                    }
-                    d_in = w;
+                d_in = dcur.x & 0xffffu;
+                dcur.x = __funnelshift_r(dcur.x, dcur.y, 16);
+                dcur.y = __funnelshift_r(dcur.y, dcur.z, 16);
+                dcur.z = __funnelshift_r(dcur.z, dcur.w, 16);
+                dcur.w >>= 16;
+                if (pass > 0) {
+                    h_in = bq0.x;
+                    f_in = bq0.y;
+                    bq0 = bq1;
+                    if (s + 2 < ncols)
+                        bq1 = a.bnd[(size_t)off16 * 16 + 2 * (s + 2) + ((pass - 1) & 1)];
                 }
+                // the next pair's table entry, once its claim has returned
+                if (pass == 0 && s == (ncols < 9 ? ncols - 1 : 8) && next < pair_count)
+                    ninfo = a.pairs[a.pair_begin + next];
             }
         }
-
-        const uint32_t d_top = d_in;
-        const bool top_valid = (d_top & kValid) != 0, bot_valid = (d_bot & kValid) != 0;
-        const bool top_first = (d_top & kFirst) != 0, bot_first = (d_bot & kFirst) != 0;
-        // resets at a segment's first column (warp-uniform branch, rare)
-        if (__any_sync(FULL, top_first || bot_first)) {
-#pragma unroll
-            for (int k = 0; k < HALF; ++k) {
-                H[k] = top_first ? Z : H[k];
-                E[k] = top_first ? Z : E[k];
-            }
-#pragma unroll
-            for (int k = HALF; k < R; ++k) {
-                H[k] = bot_first ? Z : H[k];
-                E[k] = bot_first ? Z : E[k];
-            }
-            if (top_first) prev_h = Z;
-            if (bot_first) {
-                mid_h = Z;
-                col_bot = 0;
-            }
-            if (top_first && (d_top & kFirstPass)) S_top = Z;
-            if (bot_first && (d_bot & kFirstPass)) S_bot = Z;
-        }
-        const uint32_t bot_diag = mid_h, bot_f_in = mid_f, topfin = S_topfin;
-        uint32_t f_top = f_in, f_bot = bot_f_in;
-        if (top_valid | bot_valid) {
-            // a half without a real column runs on zero-score residues: like a
-            // trailing padding column it cannot raise any score, and its rows
-            // are reset before they are used again
-            const uint32_t wt = top_valid ? d_top : kPadPair;
+        const int ct = s - 2 * t;            // top half's column
+        const bool top_valid = ct >= 0 && ct < ncols;
+        const bool bot_valid = ct >= 1 && ct <= ncols;
+        if (!done && (ct >= 0 && ct <= ncols)) {
+            // a half outside the pass's columns runs on zero-score residues:
+            // like a trailing padding column it cannot raise any score
+            const uint32_t wt = top_valid ? d_in : kPadPair;
             const uint32_t wb = bot_valid ? d_bot : kPadPair;
-            const int pt = (int)(wt >> kPassShift), pb = (int)(wb >> kPassShift);
-            const uint2* t0 = prof + ((pt * NJ) * kCodes + (int)(wt & 0xffu)) * SLOTS + slot;
-            const uint2* t1 = prof + ((pt * NJ) * kCodes + (int)((wt >> 8) & 0xffu)) * SLOTS + slot;
-            const uint2* b0 = prof + ((pb * NJ) * kCodes + (int)(wb & 0xffu)) * SLOTS + slot;
-            const uint2* b1 = prof + ((pb * NJ) * kCodes + (int)((wb >> 8) & 0xffu)) * SLOTS + slot;
-            // the top's last row before this column: the bottom's diagonal next step
-            mid_h = H[HALF - 1];
+            const uint2* prof_p = prof + (pass * NJ) * JSTRIDE + slot;
+            const uint2* t0 = prof_p + (int)(wt & 0xffu) * SLOTS;
+            const uint2* t1 = prof_p + (int)((wt >> 8) & 0xffu) * SLOTS;
+            const uint2* b0 = prof_p + (int)(wb & 0xffu) * SLOTS;
+            const uint2* b1 = prof_p + (int)((wb >> 8) & 0xffu) * SLOTS;
+            const uint32_t bot_diag = mid_h;
+            uint32_t f_top = f_in, f_bot = mid_f;
+            mid_h = H[HALF - 1];     // the top's last row one column back
             reverse_sweep<R, 0, HALF>(H, E, t0, t1, JSTRIDE, prev_h);
             reverse_sweep<R, HALF, R>(H, E, b0, b1, JSTRIDE, bot_diag);
 #pragma unroll
             for (int i = 0; i < HALF; ++i) {
                 forward_cell(H[i], E[i], f_top, K);
                 forward_cell(H[HALF + i], E[HALF + i], f_bot, K);
-                if (i & 1) {
-                    S_top = __vimax3_s16x2(S_top, H[i - 1], H[i]);
-                    S_bot = __vimax3_s16x2(S_bot, H[HALF + i - 1], H[HALF + i]);
-                } else if (i == HALF - 1) {
-                    S_top = __vimax3_s16x2(S_top, H[i], Z);
-                    S_bot = __vimax3_s16x2(S_bot, H[HALF + i], Z);
-                }
+                if (i & 1) S = __vimax3_s16x2(S, H[i - 1], H[i]);
+                if (i & 1) S = __vimax3_s16x2(S, H[HALF + i - 1], H[HALF + i]);
+                if (!(i & 1) && i == HALF - 1) S = __vimax3_s16x2(S, H[i], H[HALF + i]);
+            }
+            mid_f = f_top;
+            if (bot_valid) {
+                out_h = H[R - 1];
+                out_f = f_bot;
+                if (t == T - 1 && pass + 1 < P)
+                    a.bnd[(size_t)off16 * 16 + 2 * (ct - 1) + (pass & 1)] = make_uint2(out_h, out_f);
             }
         }
-        mid_f = f_top;
-        if (top_valid && (d_top & kLast) && (d_top & kLastPass))
-            S_topfin = __vimax3_s16x2(S_top, s_in, Z);
-        if (bot_valid) {
-            out_h = H[R - 1];
-            out_f = f_bot;
-            const int pb = (int)(d_bot >> kPassShift);
-            if (t == T - 1 && !(d_bot & kLastPass))
-                a.bnd[(size_t)o_bot * 16 + 2 * col_bot + (pb & 1)] = make_uint2(out_h, out_f);
-            if ((d_bot & kLast) && (d_bot & kLastPass)) {
-                out_s = __vimax3_s16x2(S_bot, topfin, Z);
-                if (t == T - 1) {
-                    const int pos = 2 * (a.pair_begin + (int)p_bot);
-                    const int s0 = lo16(out_s), s1 = hi16(out_s);
+        prev_h = h_in;
+        d_out = d_bot;
+        d_bot = d_in;
+        ++s;
+        if (!done && s == nsteps) {  // uniform within the group
+            __syncwarp(gmask);
+            if (pass + 1 < P) {
+                ++pass;
+                SWB_START_PASS()
+            } else {
+#pragma unroll
+                for (int o = T / 2; o > 0; o >>= 1)
+                    S = __vimax3_s16x2(S, __shfl_xor_sync(gmask, S, o, T), Z);
+                if (t == 0) {
+                    const int pos = 2 * (a.pair_begin + pair);
+                    const int s0 = lo16(S), s1 = hi16(S);
                     a.scores[pos] = s0 - bias;
                     if (s0 >= a.ovf_thresh) a.ovf_list[atomicAdd(a.ovf_count, 1)] = pos;
                     if (pos + 1 < a.n_records) {
@@ -392,19 +342,15 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
                         if (s1 >= a.ovf_thresh) a.ovf_list[atomicAdd(a.ovf_count, 1)] = pos + 1;
                     }
                 }
+                const int v = __shfl_sync(gmask, next, 0, T);
+                off16 = __shfl_sync(gmask, ninfo.off16, 0, T);
+                ncols = (int)__shfl_sync(gmask, ninfo.ncols, 0, T);
+                SWB_TAKE_PAIR(v)
             }
-            ++col_bot;
         }
-        if (d_bot & kDone) finished = true;
-        prev_h = h_in;
-        d_out = d_bot;
-        o_out = o_bot;
-        p_out = p_bot;
-        d_bot = d_top;
-        o_bot = o_in;
-        p_bot = p_in;
-        __syncwarp();   // orders thread T-1's boundary stores before later feeder loads
     }
+#undef SWB_TAKE_PAIR
+#undef SWB_START_PASS
 }
 
 }  // namespace swb
