@@ -28,7 +28,7 @@ EXPORTS = [
     "sw_last_error", "sw_db_load", "sw_db_stats_get", "sw_search",
     "sw_search_device", "sw_set_kernel_config", "sw_get_kernel_config",
     "sw_get_run_stats", "sw_set_stream", "sw_sync", "sw_reset_totals", "sw_get_totals",
-    "sw_set_tuning",
+    "sw_set_tuning", "sw_score_noalloc",
 ]
 
 
@@ -132,6 +132,10 @@ def load(path: str = LIB_PATH):
     L.sw_get_totals.argtypes = [P, ctypes.POINTER(sw_totals)]
     L.sw_set_tuning.restype = ctypes.c_int
     L.sw_set_tuning.argtypes = [P, ctypes.POINTER(sw_tuning_entry), ctypes.c_uint32]
+    L.sw_score_noalloc.restype = ctypes.c_int
+    L.sw_score_noalloc.argtypes = [ctypes.c_int, ctypes.POINTER(sw_params), ctypes.c_void_p,
+                                   ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
+                                   ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]
     _lib = L
     return L
 
@@ -149,6 +153,15 @@ def default_params(gap_open=10, gap_extend=2, top_k=10, matrix=None,
         for i in range(1024):
             p.matrix[i] = int(m[i])
     return p
+
+
+def score_noalloc(device: int, params: sw_params, d_query: int, qlen: int, d_residues: int,
+                  d_offsets: int, n_records: int, d_scores: int, stream: int | None = None) -> int:
+    """sw_score_noalloc on device pointers (ints); returns the sw_status."""
+    return load().sw_score_noalloc(device, ctypes.byref(params), ctypes.c_void_p(d_query), qlen,
+                                   ctypes.c_void_p(d_residues), ctypes.c_void_p(d_offsets),
+                                   n_records, ctypes.c_void_p(d_scores),
+                                   ctypes.c_void_p(stream) if stream else None)
 
 
 def _ptr(a: np.ndarray):
