@@ -63,9 +63,10 @@ typedef struct sw_hit {
 } sw_hit;
 
 /* Kernel shape.  group_width threads cooperate on one pair of DB records
- * (1 = one pair per thread, "inter-sequence"; 2..32 = warp-cooperative
- * anti-diagonal wavefront, "intra-sequence"); rows_per_thread query rows are
- * kept in registers per thread.  Pairs of records with more than cutover
+ * (4..32 threads, a warp-cooperative anti-diagonal wavefront; narrow groups
+ * behave like the reference's one-record-per-thread "inter-sequence" form,
+ * wide groups are the "intra-sequence" form); rows_per_thread query rows are
+ * kept in registers per thread (an even number).  Pairs of records with more than cutover
  * columns use the long shape, the rest the short shape. */
 typedef struct sw_kernel_config {
     int32_t long_group_width;
@@ -158,6 +159,11 @@ typedef struct sw_tuning_entry {
 } sw_tuning_entry;
 
 sw_status sw_set_tuning(struct sw_ctx *ctx, const sw_tuning_entry *entries, uint32_t n);
+
+/* The compiled kernel shapes: fills up to capacity (group width, rows per
+ * thread) entries; *n_shapes receives the total. */
+sw_status sw_get_shapes(int32_t *group_width, int32_t *rows_per_thread, uint32_t capacity,
+                        uint32_t *n_shapes);
 
 /* Shape the library would pick for a query of this length. */
 sw_status sw_get_kernel_config(struct sw_ctx *ctx, uint32_t qlen, sw_kernel_config *cfg);

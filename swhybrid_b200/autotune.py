@@ -21,8 +21,8 @@ import numpy as np
 
 from . import capi, synth
 
-GROUP_WIDTHS = (1, 2, 4, 8, 16, 32)
-ROWS = (8, 16, 24, 32, 40, 48, 56, 64)
+GROUP_WIDTHS = (4, 8, 16, 32)
+ROWS = (4, 6, 8, 10, 12, 16, 20, 24, 28, 32, 40, 48, 56, 64)
 DEFAULT_TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuned", "b200.json")
 
 

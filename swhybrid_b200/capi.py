@@ -28,7 +28,7 @@ EXPORTS = [
     "sw_last_error", "sw_db_load", "sw_db_stats_get", "sw_search",
     "sw_search_device", "sw_set_kernel_config", "sw_get_kernel_config",
     "sw_get_run_stats", "sw_set_stream", "sw_sync", "sw_reset_totals", "sw_get_totals",
-    "sw_set_tuning", "sw_score_noalloc",
+    "sw_set_tuning", "sw_score_noalloc", "sw_get_shapes",
 ]
 
 
@@ -132,6 +132,9 @@ def load(path: str = LIB_PATH):
     L.sw_get_totals.argtypes = [P, ctypes.POINTER(sw_totals)]
     L.sw_set_tuning.restype = ctypes.c_int
     L.sw_set_tuning.argtypes = [P, ctypes.POINTER(sw_tuning_entry), ctypes.c_uint32]
+    L.sw_get_shapes.restype = ctypes.c_int
+    L.sw_get_shapes.argtypes = [ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                                ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
     L.sw_score_noalloc.restype = ctypes.c_int
     L.sw_score_noalloc.argtypes = [ctypes.c_int, ctypes.POINTER(sw_params), ctypes.c_void_p,
                                    ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
@@ -153,6 +156,17 @@ def default_params(gap_open=10, gap_extend=2, top_k=10, matrix=None,
         for i in range(1024):
             p.matrix[i] = int(m[i])
     return p
+
+
+def shapes() -> list:
+    """Compiled (group width, rows per thread) shapes."""
+    L = load()
+    n = ctypes.c_uint32(0)
+    L.sw_get_shapes(None, None, 0, ctypes.byref(n))
+    T = (ctypes.c_int32 * n.value)()
+    R = (ctypes.c_int32 * n.value)()
+    L.sw_get_shapes(T, R, n.value, ctypes.byref(n))
+    return [(T[i], R[i]) for i in range(n.value)]
 
 
 def score_noalloc(device: int, params: sw_params, d_query: int, qlen: int, d_residues: int,

@@ -30,10 +30,6 @@
 #include "sw_registry.h"
 
 namespace swb {
-extern const WfKernel wf_table_t1[];
-extern const int wf_table_t1_n;
-extern const WfKernel wf_table_t2[];
-extern const int wf_table_t2_n;
 extern const WfKernel wf_table_t4[];
 extern const int wf_table_t4_n;
 extern const WfKernel wf_table_t8[];
@@ -48,8 +44,6 @@ const WfKernel* wf_kernels(int* n) {
     static std::once_flag once;
     std::call_once(once, [] {
         auto add = [](const WfKernel* t, int m) { all.insert(all.end(), t, t + m); };
-        add(wf_table_t1, wf_table_t1_n);
-        add(wf_table_t2, wf_table_t2_n);
         add(wf_table_t4, wf_table_t4_n);
         add(wf_table_t8, wf_table_t8_n);
         add(wf_table_t16, wf_table_t16_n);
@@ -493,6 +487,19 @@ extern "C" sw_status sw_get_kernel_config(sw_ctx* ctx, uint32_t qlen, sw_kernel_
     if (!ctx || !cfg) return SW_ERR_INVALID;
     if (!ctx->db_loaded) SW_SET(ctx, SW_ERR_STATE, "no DB loaded");
     *cfg = choose_config(ctx, (int)std::max<uint32_t>(qlen, 1));
+    return SW_OK;
+}
+
+extern "C" sw_status sw_get_shapes(int32_t* group_width, int32_t* rows_per_thread,
+                                   uint32_t capacity, uint32_t* n_shapes) {
+    if (!n_shapes) return SW_ERR_INVALID;
+    int n = 0;
+    const WfKernel* k = wf_kernels(&n);
+    *n_shapes = (uint32_t)n;
+    for (uint32_t i = 0; i < capacity && i < (uint32_t)n; ++i) {
+        if (group_width) group_width[i] = k[i].T;
+        if (rows_per_thread) rows_per_thread[i] = k[i].R;
+    }
     return SW_OK;
 }
 

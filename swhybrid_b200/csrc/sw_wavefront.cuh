@@ -53,7 +53,7 @@ struct GroupShape {
 // Shared-memory bytes of the query profile for a query of qlen rows.
 template <int T, int R>
 __host__ __device__ constexpr size_t wf_smem_bytes(int qlen) {
-    return (size_t)((qlen + T * R - 1) / (T * R)) * (R / 8) * kCodes *
+    return (size_t)((qlen + T * R - 1) / (T * R)) * ((R + 7) / 8) * kCodes *
            GroupShape<T>::SLOTS * sizeof(uint2);
 }
 
@@ -137,8 +137,8 @@ __device__ __forceinline__ void forward_cell(uint32_t& Hk, uint32_t& Ek, uint32_
 
 template <int T, int R, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
-    static_assert(R % 8 == 0 && R >= 8, "R");
-    constexpr int NJ = R / 8;
+    static_assert(R % 2 == 0 && R >= 4, "R");
+    constexpr int NJ = (R + 7) / 8;    // 8-row profile chunks per thread (last one partial)
     constexpr int HALF = R / 2;
     constexpr int SLOTS = GroupShape<T>::SLOTS;
     constexpr int JSTRIDE = kCodes * SLOTS;
