@@ -65,6 +65,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--config", type=str, default=None,
                     help="force a kernel shape 'T,R,T,R,cutover'")
+    ap.add_argument("--no-batched", action="store_true",
+                    help="skip the batched (64-query) measurement")
     ap.add_argument("--kernel-only", action="store_true",
                     help="time the resident path only (no e2e, probe or CPU baseline)")
     return ap.parse_args()
@@ -338,6 +340,51 @@ def run_ours(args, rank, world, local_rank):
     e2e_s_max = max_over_ranks(e2e_s)
     e2e_value = cells_step * args.steps * world / e2e_s_max / 1e9
 
+    # ---- batched: 64 queries, lengths log-uniform 50..5,000, one call ----
+    batched = None
+    if args.workload == "full" and not args.no_batched:
+        from swhybrid_b200 import synth as _synth
+        bq = _synth.batched_queries(3, 64, 50, 5000)
+        bcells = sum(len(q) for q in bq) * db.total
+        ctx.search_batch(bq)                       # capture the graph
+        ctx.search_batch(bq)
+        barrier()
+        torch.cuda.synchronize()
+        ev_b0 = []
+        t0 = time.perf_counter()
+        bdev = 0.0
+        for _ in range(args.steps):
+            ctx.search_batch(bq)
+            bdev += ctx.run_stats().kernel_ms
+        b_wall = time.perf_counter() - t0
+        barrier()
+        bdev_max = max_over_ranks(bdev)
+        b_wall_max = max_over_ranks(b_wall)
+        # the same 64 queries through the plain one-query-per-call path
+        ctx.set_stream(stream.cuda_stream)
+        dbq = [torch.from_numpy(q.copy()).to(f"cuda:{local_rank}") for q in bq]
+        pev0 = torch.cuda.Event(enable_timing=True)
+        pev1 = torch.cuda.Event(enable_timing=True)
+        pev0.record(stream)
+        for q in dbq:
+            ctx.search_device(q.data_ptr(), q.numel())
+        pev1.record(stream)
+        ctx.sync()
+        torch.cuda.synchronize()
+        plain_ms = max_over_ranks(pev0.elapsed_time(pev1))
+        ctx.set_stream(None)
+        batched = {
+            "workload": "64 queries, lengths log-uniform 50..5,000 (seeded), full-size DB, "
+                        "one sw_search_batch call (CUDA graph replay)",
+            "value": round(bcells * args.steps * world / (bdev_max * 1e-3) / 1e9, 3),
+            "e2e_value": round(bcells * args.steps * world / b_wall_max / 1e9, 3),
+            "unit": "GCUPS",
+            "ms_per_batch": round(bdev_max / args.steps, 3),
+            "plain_same_queries_gcups": round(bcells * world / (plain_ms * 1e-3) / 1e9, 3),
+            "speedup_vs_plain": round((bcells / (bdev_max / args.steps)) / (bcells / plain_ms), 3),
+            "launches_per_batch": int(ctx.run_stats().launches),
+        }
+
     # ---- correctness spot check on the resident DB (rank 0, cheap) ----
     spot = None
     if rank == 0 and args.workload == "small":
@@ -401,6 +448,8 @@ def run_ours(args, rank, world, local_rank):
         }
         if spot is not None:
             line["parity_spot_check"] = spot
+        if batched is not None:
+            line["batched"] = batched
     ctx.close()
     return line, db, queries
 

@@ -193,6 +193,33 @@ sw_status sw_sync(struct sw_ctx *ctx);
 sw_status sw_reset_totals(struct sw_ctx *ctx);
 sw_status sw_get_totals(const struct sw_ctx *ctx, sw_totals *out);
 
+/* ---- batched search: many queries per call -------------------------------- */
+
+/* No reference counterpart (the reference searches one query per run;
+ * WorkerPool balances DB chunks over host threads, src/WorkerPool.cpp:10-82).
+ * Options of sw_search_batch: pairs of records longer than cutover columns run
+ * in a concurrent launch with the given shape (0 = no split); use_graph != 0
+ * captures each batch signature (query count and lengths) as a CUDA graph and
+ * replays it. */
+typedef struct sw_batch_options {
+    int32_t cutover;
+    int32_t long_group_width;
+    int32_t long_rows_per_thread;
+    int32_t use_graph;
+} sw_batch_options;
+
+/* NULL restores the defaults (cut-over 8192, long shape 32x16, graphs on). */
+sw_status sw_set_batch_options(struct sw_ctx *ctx, const sw_batch_options *opt);
+
+/* Searches n_queries queries (codes back to back; query_offsets has
+ * n_queries+1 entries) against the resident DB in one device pass.
+ * hits: n_queries * top_k entries (query q's list at q * top_k); n_hits:
+ * n_queries counts; scores: optional n_queries * n_records (query-major).
+ * Results equal n_queries calls of sw_search. */
+sw_status sw_search_batch(struct sw_ctx *ctx, uint32_t n_queries, const uint8_t *queries,
+                          const uint64_t *query_offsets, sw_hit *hits, uint32_t *n_hits,
+                          int32_t *scores);
+
 /* ---- scoring without allocation ------------------------------------------ */
 
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc

@@ -28,7 +28,8 @@ EXPORTS = [
     "sw_last_error", "sw_db_load", "sw_db_stats_get", "sw_search",
     "sw_search_device", "sw_set_kernel_config", "sw_get_kernel_config",
     "sw_get_run_stats", "sw_set_stream", "sw_sync", "sw_reset_totals", "sw_get_totals",
-    "sw_set_tuning", "sw_score_noalloc", "sw_get_shapes",
+    "sw_set_tuning", "sw_score_noalloc", "sw_get_shapes", "sw_set_batch_options",
+    "sw_search_batch",
 ]
 
 
@@ -57,6 +58,11 @@ class sw_kernel_config(ctypes.Structure):
     def as_tuple(self):
         return (self.long_group_width, self.long_rows_per_thread, self.short_group_width,
                 self.short_rows_per_thread, self.cutover)
+
+
+class sw_batch_options(ctypes.Structure):
+    _fields_ = [("cutover", ctypes.c_int32), ("long_group_width", ctypes.c_int32),
+                ("long_rows_per_thread", ctypes.c_int32), ("use_graph", ctypes.c_int32)]
 
 
 class sw_tuning_entry(ctypes.Structure):
@@ -132,6 +138,11 @@ def load(path: str = LIB_PATH):
     L.sw_get_totals.argtypes = [P, ctypes.POINTER(sw_totals)]
     L.sw_set_tuning.restype = ctypes.c_int
     L.sw_set_tuning.argtypes = [P, ctypes.POINTER(sw_tuning_entry), ctypes.c_uint32]
+    L.sw_set_batch_options.restype = ctypes.c_int
+    L.sw_set_batch_options.argtypes = [P, ctypes.POINTER(sw_batch_options)]
+    L.sw_search_batch.restype = ctypes.c_int
+    L.sw_search_batch.argtypes = [P, ctypes.c_uint32, P, P, ctypes.POINTER(sw_hit),
+                                  ctypes.POINTER(ctypes.c_uint32), P]
     L.sw_get_shapes.restype = ctypes.c_int
     L.sw_get_shapes.argtypes = [ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
                                 ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
@@ -250,6 +261,29 @@ class Context:
             return
         c = sw_kernel_config(*cfg)
         self._check(self.L.sw_set_kernel_config(self.h, ctypes.byref(c)), "sw_set_kernel_config")
+
+    def set_batch_options(self, cutover=8192, long_shape=(32, 16), use_graph=True):
+        o = sw_batch_options(cutover, long_shape[0], long_shape[1], 1 if use_graph else 0)
+        self._check(self.L.sw_set_batch_options(self.h, ctypes.byref(o)), "sw_set_batch_options")
+
+    def search_batch(self, queries, want_scores: bool = False):
+        """queries: list of code arrays.  Returns (list of hit lists, scores
+        [n_queries, n_records] or None)."""
+        nq = len(queries)
+        off = np.zeros(nq + 1, dtype=np.uint64)
+        off[1:] = np.cumsum([len(q) for q in queries])
+        flat = (np.concatenate([np.asarray(q, dtype=np.uint8) for q in queries])
+                if nq and off[-1] else np.zeros(1, dtype=np.uint8))
+        k = self.params.top_k
+        hits = (sw_hit * max(nq * k, 1))()
+        nh = (ctypes.c_uint32 * max(nq, 1))()
+        scores = np.zeros((nq, max(self.n_records, 1)), dtype=np.int32) if want_scores else None
+        self._check(self.L.sw_search_batch(self.h, nq, _ptr(flat), _ptr(off), hits, nh,
+                                           _ptr(scores) if want_scores else None),
+                    "sw_search_batch")
+        out = [[(hits[q * k + i].score, hits[q * k + i].index) for i in range(nh[q])]
+               for q in range(nq)]
+        return out, (scores[:, :self.n_records] if want_scores else None)
 
     def set_tuning(self, table):
         """table: [(max_qlen, (T, R, T, R, cutover)), ...] sorted by max_qlen."""

@@ -18,10 +18,10 @@ constexpr int kRsRows = 16;        // query rows per lane in the 32-bit pass
 
 // One warp per overflowed record: the same anti-diagonal wavefront as the
 // first pass (32 lanes x 16 rows per pass), int32 arithmetic, profile taken
-// from a shared copy of the matrix.  The record's boundary row between passes
-// uses the pair's boundary buffer half that belongs to its lane, so two
-// records of one pair can be re-scored concurrently.
-__global__ void __launch_bounds__(256) sw_rescore32(const RescoreArgs a) {
+// from a shared copy of the matrix.  The boundary row between query passes is
+// the warp's own scratch row, so any two records (of the same or of
+// different queries) can be re-scored concurrently.
+__global__ void __launch_bounds__(64) sw_rescore32(const RescoreArgs a) {
     __shared__ int smat[32 * 32];
     for (int i = threadIdx.x; i < 1024; i += blockDim.x) smat[i] = a.mat[i];
     __syncthreads();
@@ -29,24 +29,32 @@ __global__ void __launch_bounds__(256) sw_rescore32(const RescoreArgs a) {
     const int lane = threadIdx.x & 31;
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    uint2* pb = a.scratch + (size_t)warp * a.max_cols;
     const int count = *a.ovf_count;
     for (int it = warp; it < count; it += nwarps) {
-        const int pos = a.ovf_list[it];
+        const int entry = a.ovf_list[it];
+        int pos = entry;
+        const uint8_t* query = a.query;
+        int qlen = a.qlen;
+        if (a.qoff) {
+            const int q = entry / a.n_records;
+            pos = entry - q * a.n_records;
+            query = a.queries + a.qoff[q];
+            qlen = (int)a.qlens[q];
+        }
         const Pair2 pr = a.pairs[pos >> 1];
         const int sel = pos & 1;
         const uint8_t* seq = reinterpret_cast<const uint8_t*>(a.db + pr.off16);
         const int ncols = (int)pr.ncols;
-        const int ncols_pad = (ncols + 7) & ~7;
-        uint2* pb = a.bnd + (size_t)pr.off16 * 16 + (size_t)sel * ncols_pad;
         const int rows_per_pass = 32 * kRsRows;
-        const int P = (a.qlen + rows_per_pass - 1) / rows_per_pass;
+        const int P = (qlen + rows_per_pass - 1) / rows_per_pass;
         int S = 0;
         for (int pass = 0; pass < P; ++pass) {
             int qc[kRsRows], H[kRsRows], E[kRsRows];
 #pragma unroll
             for (int k = 0; k < kRsRows; ++k) {
                 const int row = pass * rows_per_pass + lane * kRsRows + k;
-                qc[k] = (row < a.qlen) ? (int)(a.query[row] & 31) * 32 : kZeroCode * 32;
+                qc[k] = (row < qlen) ? (int)(query[row] & 31) * 32 : kZeroCode * 32;
                 H[k] = 0;
                 E[k] = 0;
             }
@@ -94,7 +102,7 @@ __global__ void __launch_bounds__(256) sw_rescore32(const RescoreArgs a) {
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) S = max(S, __shfl_xor_sync(FULL, S, o));
-        if (lane == 0) a.scores[pos] = S;
+        if (lane == 0) a.scores[entry] = S;
         __syncwarp();
     }
 }
@@ -107,17 +115,18 @@ __global__ void __launch_bounds__(256) sw_rescore32(const RescoreArgs a) {
 __global__ void __launch_bounds__(kTopkThreads) sw_topk_round(const TopkArgs a) {
     __shared__ unsigned long long sk[kTopkKeys];
     const long long base = (long long)blockIdx.x * kTopkKeys;
+    const long long y = blockIdx.y;                 // query of a batch
     for (int i = threadIdx.x; i < kTopkKeys; i += kTopkThreads) {
         const long long g = base + i;
         unsigned long long key = 0ull;
         if (g < a.n) {
             if (a.keys_in) {
-                key = a.keys_in[g];
+                key = a.keys_in[y * a.in_stride + g];
             } else {
-                int s = a.scores[g];
+                int s = a.scores[y * a.in_stride + g];
                 if (a.cap && s > 65535) s = 65535;
                 const uint32_t rec = a.perm[g];
-                if (a.scores_by_record) a.scores_by_record[rec] = s;
+                if (a.scores_by_record) a.scores_by_record[y * a.rec_stride + rec] = s;
                 if (s > 0) key = ((unsigned long long)(uint32_t)s << 32) | (0xffffffffu - rec);
             }
         }
@@ -140,7 +149,7 @@ __global__ void __launch_bounds__(kTopkThreads) sw_topk_round(const TopkArgs a) 
         }
     }
     for (int i = threadIdx.x; i < a.k; i += kTopkThreads)
-        a.keys_out[(long long)blockIdx.x * a.k + i] = sk[i];
+        a.keys_out[y * a.out_stride + (long long)blockIdx.x * a.k + i] = sk[i];
 }
 
 }  // namespace swb

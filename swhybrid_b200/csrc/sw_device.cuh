@@ -48,6 +48,31 @@ struct WfArgs {
     int ovf_thresh;             // biased lane value >= this may have wrapped
 };
 
+// Arguments of the batched first-pass kernel (sw_wavefront.cuh, sw_batch).
+struct BatchArgs {
+    const uint4* db;
+    const Pair2* pairs;
+    int pair_begin;             // pairs [pair_begin, pair_begin + pair_count) of every query
+    int pair_count;
+    const uint8_t* queries;     // all queries' codes back to back
+    const uint32_t* qoff;       // per query: offset into queries
+    const uint32_t* qlen;       // per query: length
+    const int* qlist;           // the queries of this launch, in order
+    int nq;
+    int* counters;              // one pair counter per entry of qlist (zero before)
+    const int8_t* mat;
+    uint32_t bias2;
+    uint32_t neg_e;
+    uint32_t one;
+    uint2* bnd;                 // per-group boundary rows
+    size_t bnd_group;           // entries per group (2 per column of the longest pair)
+    int* scores;                // [query][sorted position]
+    int n_records;
+    int* ovf_list;              // query * n_records + position
+    int* ovf_count;
+    int ovf_thresh;
+};
+
 __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {
     uint32_t r;
     asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(sel));

@@ -65,40 +65,7 @@ const WfKernel* find_kernel(int T, int R) {
 
 using namespace swb;
 
-// ---------------------------------------------------------------------------
-// errors
-// ---------------------------------------------------------------------------
-
-#define SW_SET(ctx, code, ...)                                              \
-    do {                                                                    \
-        char _b[512];                                                       \
-        snprintf(_b, sizeof(_b), __VA_ARGS__);                              \
-        if (ctx) (ctx)->err = _b;                                           \
-        return code;                                                        \
-    } while (0)
-
-#define SW_CUDA(ctx, call)                                                  \
-    do {                                                                    \
-        cudaError_t _e = (call);                                            \
-        if (_e != cudaSuccess)                                              \
-            SW_SET(ctx, SW_ERR_CUDA, "%s failed: %s (%s:%d)", #call,        \
-                   cudaGetErrorString(_e), __FILE__, __LINE__);             \
-    } while (0)
-
 namespace {
-
-template <typename T>
-cudaError_t dev_alloc(T** p, size_t count) {
-    *p = nullptr;
-    if (count == 0) count = 1;
-    return cudaMalloc((void**)p, count * sizeof(T));
-}
-
-template <typename T>
-void dev_free(T*& p) {
-    if (p) cudaFree((void*)p);
-    p = nullptr;
-}
 
 double now_ms() {
     return std::chrono::duration<double, std::milli>(
@@ -248,6 +215,8 @@ extern "C" sw_status sw_ctx_create(int device, const sw_params* params, sw_ctx**
 }
 
 static void free_db(sw_ctx* ctx) {
+    swb::free_batch(ctx);
+    dev_free(ctx->d_rs_scratch);
     dev_free(ctx->d_db);
     dev_free(ctx->d_pairs);
     dev_free(ctx->d_perm);
@@ -334,6 +303,9 @@ extern "C" sw_status sw_db_load(sw_ctx* ctx, const uint8_t* residues, const uint
         if (nc > 0) nonempty = p + 1;
         if (units >= (1ull << 32)) SW_SET(ctx, SW_ERR_UNSUPPORTED, "DB too large for 32-bit unit offsets");
     }
+    int max_cols = 8;
+    for (uint64_t p = 0; p < npairs_all; ++p)
+        max_cols = std::max(max_cols, (int)((pairs[p].ncols + 7) / 8 * 8));
     std::vector<uint8_t> stream((size_t)units * 16, (uint8_t)kZeroCode);
     for (uint64_t p = 0; p < npairs_all; ++p) {
         uint8_t* dst = stream.data() + (size_t)pairs[p].off16 * 16;
@@ -367,6 +339,9 @@ extern "C" sw_status sw_db_load(sw_ctx* ctx, const uint8_t* residues, const uint
     if (dev_alloc(&ctx->d_scores, n + 1) != cudaSuccess) return nomem("scores");
     if (dev_alloc(&ctx->d_scores_rec, n + 1) != cudaSuccess) return nomem("scores");
     if (dev_alloc(&ctx->d_ovf, n + 1) != cudaSuccess) return nomem("overflow list");
+    ctx->max_cols = max_cols;
+    if (dev_alloc(&ctx->d_rs_scratch, (size_t)kRescoreWarps * max_cols) != cudaSuccess)
+        return nomem("re-score rows");
     const size_t nblk = (n + kTopkKeys - 1) / kTopkKeys + 1;
     if (dev_alloc(&ctx->d_keys[0], nblk * kMaxTopK) != cudaSuccess) return nomem("keys");
     if (dev_alloc(&ctx->d_keys[1], nblk * kMaxTopK) != cudaSuccess) return nomem("keys");
@@ -630,12 +605,17 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
         r.mat = ctx->d_mat;
         r.gap_oe = ctx->params.gap_open + ctx->params.gap_extend;
         r.gap_e = ctx->params.gap_extend;
+        r.queries = nullptr;
+        r.qoff = nullptr;
+        r.qlens = nullptr;
+        r.n_records = (int)ctx->n_records;
         r.ovf_list = ctx->d_ovf;
         r.ovf_count = ctx->d_counters + 2;
-        r.bnd = ctx->d_bnd;
+        r.scratch = ctx->d_rs_scratch;
+        r.max_cols = ctx->max_cols;
         r.scores = ctx->d_scores;
         void* args[] = {&r};
-        SW_CUDA(ctx, cudaLaunchKernel((const void*)sw_rescore32, dim3(ctx->num_sms), dim3(256),
+        SW_CUDA(ctx, cudaLaunchKernel((const void*)sw_rescore32, dim3(kRescoreBlocks), dim3(64),
                                       args, 0, st));
         ++*launches;
     }
@@ -656,6 +636,9 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
         t.cap = (ctx->params.flags & SW_FLAG_REFERENCE_CAP) ? 1 : 0;
         t.scores_by_record = first ? d_scores_rec : nullptr;
         t.keys_out = ctx->d_keys[buf];
+        t.in_stride = 0;
+        t.rec_stride = 0;
+        t.out_stride = 0;
         void* args[] = {&t};
         SW_CUDA(ctx, cudaLaunchKernel((const void*)sw_topk_round, dim3((unsigned)blocks),
                                       dim3(kTopkThreads), args, 0, st));

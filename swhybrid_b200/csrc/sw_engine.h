@@ -1,6 +1,7 @@
 // sw_engine.h -- the context behind the C ABI's opaque sw_ctx.
 #pragma once
 #include <cstdint>
+#include <cstdio>
 #include <string>
 #include <vector>
 
@@ -8,6 +9,37 @@
 
 #include "../../include/swb200.h"
 #include "sw_device.cuh"
+
+#define SW_SET(ctx, code, ...)                                              \
+    do {                                                                    \
+        char _b[512];                                                       \
+        snprintf(_b, sizeof(_b), __VA_ARGS__);                              \
+        if (ctx) (ctx)->err = _b;                                           \
+        return code;                                                        \
+    } while (0)
+
+#define SW_CUDA(ctx, call)                                                  \
+    do {                                                                    \
+        cudaError_t _e = (call);                                            \
+        if (_e != cudaSuccess)                                              \
+            SW_SET(ctx, SW_ERR_CUDA, "%s failed: %s (%s:%d)", #call,        \
+                   cudaGetErrorString(_e), __FILE__, __LINE__);             \
+    } while (0)
+
+template <typename T>
+inline cudaError_t dev_alloc(T** p, size_t count) {
+    *p = nullptr;
+    if (count == 0) count = 1;
+    return cudaMalloc((void**)p, count * sizeof(T));
+}
+
+template <typename T>
+inline void dev_free(T*& p) {
+    if (p) cudaFree((void*)p);
+    p = nullptr;
+}
+
+struct sw_batch_state;   // batched search buffers and captured graphs (sw_batch.cu)
 
 struct sw_ctx {
     int device = 0;
@@ -50,6 +82,9 @@ struct sw_ctx {
     int* d_scores_rec = nullptr;       // per record
     int* d_ovf = nullptr;              // overflow list
     unsigned long long* d_keys[2] = {nullptr, nullptr};
+    uint2* d_rs_scratch = nullptr;     // 32-bit re-score: one boundary row per warp
+    int max_cols = 0;                  // longest pair, padded to 8 columns
+    sw_batch_state* batch = nullptr;
 
     // per-query buffers
     size_t query_cap = 0;
@@ -63,3 +98,13 @@ struct sw_ctx {
     sw_run_stats stats{};
     std::string err;
 };
+
+namespace swb {
+struct WfKernel;
+const WfKernel* find_kernel(int T, int R);
+int shape_occupancy(sw_ctx* ctx, const WfKernel& k, int qlen);
+sw_kernel_config choose_config(sw_ctx* ctx, int qlen);
+sw_status take_marks(sw_ctx* ctx, sw_ctx::Marks* m);
+sw_status drain(sw_ctx* ctx, float* last_ms, float* last_fp_ms);
+void free_batch(sw_ctx* ctx);
+}  // namespace swb

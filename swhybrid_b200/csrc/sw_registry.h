@@ -8,8 +8,9 @@ struct WfKernel {
     int T;                         // threads per record pair
     int R;                         // query rows per thread
     int block;                     // threads per block
-    const void* fn;                // __global__ sw_wavefront<T, R, block>
+    const void* fn;                // __global__ sw_wavefront<T, R, block> (plain)
     size_t (*smem)(int qlen);      // shared-memory bytes for a query length
+    const void* batch_fn;          // __global__ sw_batch<T, R, block> (batched)
 };
 
 // All instantiated shapes (sw_wf_t*.cu).

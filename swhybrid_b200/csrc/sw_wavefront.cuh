@@ -135,44 +135,70 @@ __device__ __forceinline__ void forward_cell(uint32_t& Hk, uint32_t& Ek, uint32_
     f = __viaddmax_s16x2(f, K.neg_e2, hq);
 }
 
-template <int T, int R, int BLOCK>
-__global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
+// Query profile of one query -> shared memory (whole block; the caller
+// synchronises).  Layout [pass][chunk][code][slot] of 8-byte words holding the
+// signed scores of 8 consecutive rows of the slot's thread.
+template <int T, int R>
+__device__ __forceinline__ void build_profile(uint2* prof, const uint8_t* query, int qlen,
+                                              const int8_t* mat, int P) {
+    constexpr int NJ = (R + 7) / 8;
+    constexpr int SLOTS = GroupShape<T>::SLOTS;
+    constexpr int JSTRIDE = kCodes * SLOTS;
+    const int rows_per_pass = T * R;
+    const int total = P * NJ * JSTRIDE;
+    for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
+        const int slot = idx % SLOTS;
+        int rest = idx / SLOTS;
+        const int d = rest % kCodes;
+        rest /= kCodes;
+        const int j = rest % NJ;
+        const int p = rest / NJ;
+        const int row0 = p * rows_per_pass + (slot % T) * R + j * 8;
+        uint32_t w0 = 0u, w1 = 0u;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const int row = row0 + i;
+            int v = 0;
+            if (row < qlen) v = mat[(query[row] & 31) * 32 + d];
+            const uint32_t b = (uint32_t)(uint8_t)(int8_t)v << (8 * (i & 3));
+            if (i < 4) w0 |= b; else w1 |= b;
+        }
+        prof[idx] = make_uint2(w0, w1);
+    }
+}
+
+// What one call of run_pairs works on.
+struct RunArgs {
+    const uint4* db;            // pair column streams
+    const Pair2* pairs;         // pair table, ncols descending
+    int pair_begin;             // pairs [pair_begin, pair_begin + pair_count)
+    int pair_count;
+    int* counter;               // pairs of the range claimed so far
+    int P;                      // query passes of T*R rows
+    uint32_t bias2, neg_e, one; // see CellK
+    uint2* bnd;                 // boundary rows between passes
+    size_t bnd_group;           // 0: per-pair rows at bnd + 16*off16; else this many
+                                // entries per group at bnd + group * bnd_group
+    int* scores;                // scores of this query, by sorted position
+    int n_records;
+    int* ovf_list;              // (ovf_base + position) of lanes for the 32-bit pass
+    int* ovf_count;
+    int ovf_base;
+    int ovf_thresh;             // biased lane value >= this may have wrapped
+};
+
+// The group loop: every group of T threads claims pairs from the range and
+// scores them against the query whose profile is in prof.  Returns when the
+// range is exhausted (warp-wide).
+template <int T, int R>
+__device__ __forceinline__ void run_pairs(const RunArgs& a, const uint2* prof) {
     static_assert(R % 2 == 0 && R >= 4, "R");
     constexpr int NJ = (R + 7) / 8;    // 8-row profile chunks per thread (last one partial)
     constexpr int HALF = R / 2;
     constexpr int SLOTS = GroupShape<T>::SLOTS;
     constexpr int JSTRIDE = kCodes * SLOTS;
-    extern __shared__ uint2 prof[];
-
-    const int rows_per_pass = T * R;
-    const int P = (a.qlen + rows_per_pass - 1) / rows_per_pass;
-
-    // ---- query profile -> shared memory (once per block) ----
-    {
-        const int total = P * NJ * JSTRIDE;
-        for (int idx = threadIdx.x; idx < total; idx += blockDim.x) {
-            const int slot = idx % SLOTS;
-            int rest = idx / SLOTS;
-            const int d = rest % kCodes;
-            rest /= kCodes;
-            const int j = rest % NJ;
-            const int p = rest / NJ;
-            const int row0 = p * rows_per_pass + (slot % T) * R + j * 8;
-            uint32_t w0 = 0u, w1 = 0u;
-#pragma unroll
-            for (int i = 0; i < 8; ++i) {
-                const int row = row0 + i;
-                int v = 0;
-                if (row < a.qlen) v = a.mat[(a.query[row] & 31) * 32 + d];
-                const uint32_t b = (uint32_t)(uint8_t)(int8_t)v << (8 * (i & 3));
-                if (i < 4) w0 |= b; else w1 |= b;
-            }
-            prof[idx] = make_uint2(w0, w1);
-        }
-    }
-    __syncthreads();
-
     constexpr unsigned FULL = 0xffffffffu;
+    const int P = a.P;
     const int lane = threadIdx.x & 31;
     const int t = lane & (T - 1);
     const int slot = lane & (SLOTS - 1);
@@ -185,6 +211,8 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
     const uint32_t Z = a.bias2;        // biased zero of both lanes
     const int bias = (int)(a.bias2 & 0xffffu);
     const int pair_count = a.pair_count;
+    uint2* const grp_bnd =
+        a.bnd + (size_t)((blockIdx.x * blockDim.x + threadIdx.x) / T) * a.bnd_group;
 
     // rows [0, HALF): top half, on column s - 2t; rows [HALF, R): bottom half,
     // on column s - 2t - 1 (s = step within the pass)
@@ -194,6 +222,7 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
     uint32_t d_bot = kPadPair, d_out = kPadPair;
     int pair = 0, next = 0, pass = 0, s = 0, nsteps = 0, ncols = 0;
     uint32_t off16 = 0u;
+    uint2* pbnd = grp_bnd;
     bool done = false;
     // thread 0 of a group: residue chunks (current, next), boundary entries of
     // the next two columns, and the next pair (claimed one pair ahead)
@@ -220,7 +249,7 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
             dcur = __ldg(a.db + off16);                                    \
             if (ncols > 8) dnext = __ldg(a.db + off16 + 1);                \
             if (pass > 0) {                                                \
-                const uint2* pb = a.bnd + (size_t)off16 * 16 + ((pass - 1) & 1); \
+                const uint2* pb = pbnd + ((pass - 1) & 1);                 \
                 bq0 = pb[0];                                               \
                 if (ncols > 1) bq1 = pb[2];                                \
             }                                                              \
@@ -236,6 +265,7 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
             pair = (v);                                                    \
             pass = 0;                                                      \
             S = Z;                                                         \
+            pbnd = a.bnd_group ? grp_bnd : a.bnd + (size_t)off16 * 16;     \
             if (t == 0) next = atomicAdd(a.counter, 1);                    \
             SWB_START_PASS()                                               \
         }                                                                  \
@@ -277,8 +307,7 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
                     h_in = bq0.x;
                     f_in = bq0.y;
                     bq0 = bq1;
-                    if (s + 2 < ncols)
-                        bq1 = a.bnd[(size_t)off16 * 16 + 2 * (s + 2) + ((pass - 1) & 1)];
+                    if (s + 2 < ncols) bq1 = pbnd[2 * (s + 2) + ((pass - 1) & 1)];
                 }
                 // the next pair's table entry, once its claim has returned
                 if (pass == 0 && s == (ncols < 9 ? ncols - 1 : 8) && next < pair_count)
@@ -316,7 +345,7 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
                 out_h = H[R - 1];
                 out_f = f_bot;
                 if (t == T - 1 && pass + 1 < P)
-                    a.bnd[(size_t)off16 * 16 + 2 * (ct - 1) + (pass & 1)] = make_uint2(out_h, out_f);
+                    pbnd[2 * (ct - 1) + (pass & 1)] = make_uint2(out_h, out_f);
             }
         }
         prev_h = h_in;
@@ -336,10 +365,12 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
                     const int pos = 2 * (a.pair_begin + pair);
                     const int s0 = lo16(S), s1 = hi16(S);
                     a.scores[pos] = s0 - bias;
-                    if (s0 >= a.ovf_thresh) a.ovf_list[atomicAdd(a.ovf_count, 1)] = pos;
+                    if (s0 >= a.ovf_thresh)
+                        a.ovf_list[atomicAdd(a.ovf_count, 1)] = a.ovf_base + pos;
                     if (pos + 1 < a.n_records) {
                         a.scores[pos + 1] = s1 - bias;
-                        if (s1 >= a.ovf_thresh) a.ovf_list[atomicAdd(a.ovf_count, 1)] = pos + 1;
+                        if (s1 >= a.ovf_thresh)
+                            a.ovf_list[atomicAdd(a.ovf_count, 1)] = a.ovf_base + pos + 1;
                     }
                 }
                 const int v = __shfl_sync(gmask, next, 0, T);
@@ -351,6 +382,71 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
     }
 #undef SWB_TAKE_PAIR
 #undef SWB_START_PASS
+}
+
+// Plain search: one query, the pairs of one range.
+template <int T, int R, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
+    extern __shared__ uint2 prof[];
+    const int P = (a.qlen + T * R - 1) / (T * R);
+    build_profile<T, R>(prof, a.query, a.qlen, a.mat, P);
+    __syncthreads();
+    RunArgs r;
+    r.db = a.db;
+    r.pairs = a.pairs;
+    r.pair_begin = a.pair_begin;
+    r.pair_count = a.pair_count;
+    r.counter = a.counter;
+    r.P = P;
+    r.bias2 = a.bias2;
+    r.neg_e = a.neg_e;
+    r.one = a.one;
+    r.bnd = a.bnd;
+    r.bnd_group = 0;
+    r.scores = a.scores;
+    r.n_records = a.n_records;
+    r.ovf_list = a.ovf_list;
+    r.ovf_count = a.ovf_count;
+    r.ovf_base = 0;
+    r.ovf_thresh = a.ovf_thresh;
+    run_pairs<T, R>(r, prof);
+}
+
+// Batched search: one persistent launch over a list of queries.  Every block
+// walks the list in order; for each query it rebuilds the profile in shared
+// memory and its groups claim pairs from that query's counter (the device work
+// queue), so the whole grid moves through the queries without a launch per
+// query, and a block only waits for its own groups at a query switch.
+template <int T, int R, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 1) sw_batch(const BatchArgs a) {
+    extern __shared__ uint2 prof[];
+    for (int i = 0; i < a.nq; ++i) {
+        const int q = a.qlist[i];
+        const int qlen = (int)a.qlen[q];
+        const int P = (qlen + T * R - 1) / (T * R);
+        __syncthreads();        // every group is done with the previous profile
+        build_profile<T, R>(prof, a.queries + a.qoff[q], qlen, a.mat, P);
+        __syncthreads();
+        RunArgs r;
+        r.db = a.db;
+        r.pairs = a.pairs;
+        r.pair_begin = a.pair_begin;
+        r.pair_count = a.pair_count;
+        r.counter = a.counters + i;
+        r.P = P;
+        r.bias2 = a.bias2;
+        r.neg_e = a.neg_e;
+        r.one = a.one;
+        r.bnd = a.bnd;
+        r.bnd_group = a.bnd_group;
+        r.scores = a.scores + (size_t)q * a.n_records;
+        r.n_records = a.n_records;
+        r.ovf_list = a.ovf_list;
+        r.ovf_count = a.ovf_count;
+        r.ovf_base = q * a.n_records;
+        r.ovf_thresh = a.ovf_thresh;
+        run_pairs<T, R>(r, prof);
+    }
 }
 
 }  // namespace swb

@@ -6,7 +6,8 @@ namespace swb {
 namespace {
 template <int R, int B>
 constexpr WfKernel inst() {
-    return WfKernel{16, R, B, (const void*)&sw_wavefront<16, R, B>, &wf_smem_bytes<16, R>};
+    return WfKernel{16, R, B, (const void*)&sw_wavefront<16, R, B>, &wf_smem_bytes<16, R>,
+                    (const void*)&sw_batch<16, R, B>};
 }
 }  // namespace
 

@@ -6,7 +6,8 @@ namespace swb {
 namespace {
 template <int R, int B>
 constexpr WfKernel inst() {
-    return WfKernel{32, R, B, (const void*)&sw_wavefront<32, R, B>, &wf_smem_bytes<32, R>};
+    return WfKernel{32, R, B, (const void*)&sw_wavefront<32, R, B>, &wf_smem_bytes<32, R>,
+                    (const void*)&sw_batch<32, R, B>};
 }
 }  // namespace
 

@@ -6,7 +6,8 @@ namespace swb {
 namespace {
 template <int R, int B>
 constexpr WfKernel inst() {
-    return WfKernel{4, R, B, (const void*)&sw_wavefront<4, R, B>, &wf_smem_bytes<4, R>};
+    return WfKernel{4, R, B, (const void*)&sw_wavefront<4, R, B>, &wf_smem_bytes<4, R>,
+                    (const void*)&sw_batch<4, R, B>};
 }
 }  // namespace
 

@@ -6,7 +6,8 @@ namespace swb {
 namespace {
 template <int R, int B>
 constexpr WfKernel inst() {
-    return WfKernel{8, R, B, (const void*)&sw_wavefront<8, R, B>, &wf_smem_bytes<8, R>};
+    return WfKernel{8, R, B, (const void*)&sw_wavefront<8, R, B>, &wf_smem_bytes<8, R>,
+                    (const void*)&sw_batch<8, R, B>};
 }
 }  // namespace
 

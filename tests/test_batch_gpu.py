@@ -1,0 +1,81 @@
+"""Batched search (sw_search_batch): every query's scores and top-k must equal
+what the plain per-query search returns (which is itself pinned to the
+reference's golden vectors), for every bucket/cut-over arrangement, with the
+captured CUDA graph replayed."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from swhybrid_b200 import capi, param, synth
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+M = param.blosum62()
+
+
+def load(name):
+    z = np.load(os.path.join(GOLD, name + ".npz"))
+    qo = z["qoffsets"].astype(np.int64)
+    queries = [z["queries"][qo[i]:qo[i + 1]] for i in range(len(qo) - 1)]
+    return z["residues"], z["offsets"], queries, z["scores"]
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = capi.Context(0, capi.default_params(top_k=10))
+    yield c
+    c.close()
+
+
+def test_batch_equals_golden(ctx):
+    res, off, queries, gold = load("edge")
+    ctx.load_db(res, off)
+    hits, scores = ctx.search_batch(queries, want_scores=True)
+    for qi in range(len(queries)):
+        np.testing.assert_array_equal(scores[qi], gold[qi], err_msg=f"query {qi}")
+        sc, idx = oracle.topk(gold[qi], 10)
+        assert hits[qi] == list(zip(sc.tolist(), idx.tolist()))
+
+
+@pytest.mark.parametrize("cutover", [0, 300, 1000, 4096])
+def test_batch_equals_plain_with_split(ctx, cutover):
+    rng = np.random.default_rng(41)
+    db = synth.small_db(12, 3000)
+    qs = [synth.residues(rng, int(L)) for L in (5, 31, 144, 375, 700, 1500, 2600, 60, 0)]
+    db, _ = synth.plant_homologs(rng, db, qs[4], 0.01)
+    ctx.load_db(db.residues, db.offsets)
+    ctx.set_batch_options(cutover=cutover)
+    try:
+        for rep in range(2):                # capture, then replay
+            hits, scores = ctx.search_batch(qs, want_scores=True)
+            for qi, q in enumerate(qs):
+                h1, s1 = ctx.search(q, want_scores=True)
+                np.testing.assert_array_equal(scores[qi], s1, err_msg=f"q{qi} len {len(q)}")
+                assert hits[qi] == h1
+    finally:
+        ctx.set_batch_options()
+
+
+def test_batch_saturation_and_cap():
+    res, off, queries, gold = load("saturation")
+    with capi.Context(0, capi.default_params(top_k=5)) as c:
+        c.load_db(res, off)
+        hits, scores = c.search_batch(queries, want_scores=True)
+        np.testing.assert_array_equal(scores, gold)
+
+
+def test_batch_without_graph_and_empty(ctx):
+    db = synth.small_db(13, 500)
+    ctx.load_db(db.residues, db.offsets)
+    ctx.set_batch_options(use_graph=False)
+    try:
+        qs = [synth.query(1, 100), np.zeros(0, dtype=np.uint8), synth.query(2, 333)]
+        hits, scores = ctx.search_batch(qs, want_scores=True)
+        assert hits[1] == [] and not scores[1].any()
+        for qi in (0, 2):
+            want = oracle.search(qs[qi], db.residues, db.offsets, M, 12, 2)
+            np.testing.assert_array_equal(scores[qi], want)
+    finally:
+        ctx.set_batch_options()
