@@ -208,6 +208,8 @@ extern "C" sw_status sw_ctx_create(int device, const sw_params* params, sw_ctx**
     const WfKernel* ks = wf_kernels(&nk);
     for (int i = 0; i < nk; ++i)
         if (cudaFuncSetAttribute(ks[i].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 ctx->max_smem) != cudaSuccess ||
+            cudaFuncSetAttribute(ks[i].batch_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  ctx->max_smem) != cudaSuccess)
             return fail(SW_ERR_CUDA);
     *out = ctx;
