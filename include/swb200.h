@@ -197,8 +197,12 @@ sw_status sw_get_totals(const struct sw_ctx *ctx, sw_totals *out);
 
 /* No reference counterpart (the reference searches one query per run;
  * WorkerPool balances DB chunks over host threads, src/WorkerPool.cpp:10-82).
- * Options of sw_search_batch: pairs of records longer than cutover columns run
- * in a concurrent launch with the given shape (0 = no split); use_graph != 0
+ * Options of sw_search_batch.  Queries shorter than stack_rows residues are
+ * packed several to a "stack" (rows_per_thread-aligned blocks of one virtual
+ * query) and scored by one launch of shape group_width x rows_per_thread;
+ * longer queries form stacks of their own, grouped by the shape the tuning
+ * table gives their length.  Pairs of records longer than cutover columns run
+ * in a concurrent launch with the long shape (0 = no split).  use_graph != 0
  * captures each batch signature (query count and lengths) as a CUDA graph and
  * replays it. */
 typedef struct sw_batch_options {
@@ -206,9 +210,13 @@ typedef struct sw_batch_options {
     int32_t long_group_width;
     int32_t long_rows_per_thread;
     int32_t use_graph;
+    int32_t group_width;
+    int32_t rows_per_thread;
+    int32_t stack_rows;
 } sw_batch_options;
 
-/* NULL restores the defaults (cut-over 8192, long shape 32x16, graphs on). */
+/* NULL restores the defaults (cut-over 8192, long shape 32x16, graphs on,
+ * stacks of up to 1024 rows with shape 16x32). */
 sw_status sw_set_batch_options(struct sw_ctx *ctx, const sw_batch_options *opt);
 
 /* Searches n_queries queries (codes back to back; query_offsets has

@@ -62,7 +62,9 @@ class sw_kernel_config(ctypes.Structure):
 
 class sw_batch_options(ctypes.Structure):
     _fields_ = [("cutover", ctypes.c_int32), ("long_group_width", ctypes.c_int32),
-                ("long_rows_per_thread", ctypes.c_int32), ("use_graph", ctypes.c_int32)]
+                ("long_rows_per_thread", ctypes.c_int32), ("use_graph", ctypes.c_int32),
+                ("group_width", ctypes.c_int32), ("rows_per_thread", ctypes.c_int32),
+                ("stack_rows", ctypes.c_int32)]
 
 
 class sw_tuning_entry(ctypes.Structure):
@@ -262,8 +264,10 @@ class Context:
         c = sw_kernel_config(*cfg)
         self._check(self.L.sw_set_kernel_config(self.h, ctypes.byref(c)), "sw_set_kernel_config")
 
-    def set_batch_options(self, cutover=8192, long_shape=(32, 16), use_graph=True):
-        o = sw_batch_options(cutover, long_shape[0], long_shape[1], 1 if use_graph else 0)
+    def set_batch_options(self, cutover=8192, long_shape=(32, 16), use_graph=True,
+                          stack_shape=(16, 32), stack_rows=1024):
+        o = sw_batch_options(cutover, long_shape[0], long_shape[1], 1 if use_graph else 0,
+                             stack_shape[0], stack_shape[1], stack_rows)
         self._check(self.L.sw_set_batch_options(self.h, ctypes.byref(o)), "sw_set_batch_options")
 
     def search_batch(self, queries, want_scores: bool = False):

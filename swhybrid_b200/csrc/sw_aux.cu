@@ -30,7 +30,7 @@ __global__ void __launch_bounds__(64) sw_rescore32(const RescoreArgs a) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int nwarps = (gridDim.x * blockDim.x) >> 5;
     uint2* pb = a.scratch + (size_t)warp * a.max_cols;
-    const int count = *a.ovf_count;
+    const int count = min(*a.ovf_count, a.ovf_cap);
     for (int it = warp; it < count; it += nwarps) {
         const int entry = a.ovf_list[it];
         int pos = entry;

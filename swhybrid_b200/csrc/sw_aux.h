@@ -27,6 +27,7 @@ struct RescoreArgs {
     int gap_e;
     const int* ovf_list;
     const int* ovf_count;
+    int ovf_cap;
     uint2* scratch;             // kRescoreWarps rows of max_cols entries
     int max_cols;
     int* scores;                // indexed by the overflow entry

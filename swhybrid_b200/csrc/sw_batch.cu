@@ -4,11 +4,14 @@
 // The reference has no batched mode: WorkerPool searches one query per run
 // and balances DB chunks across worker threads on the host
 // (src/WorkerPool.cpp:10-82, src/DataPool.cpp:171-286).  Here a batch is:
-//   * the queries sorted by length and cut into length buckets, one bucket per
-//     kernel shape the tuning table picks for those lengths;
-//   * per bucket, one persistent launch of sw_batch<T,R> over the bucket's
-//     queries (blocks walk the queries in order, groups claim record pairs from
-//     one device counter per query), plus, when a cut-over is set, a concurrent
+//   * queries shorter than the stack height packed (first fit, longest first)
+//     into "stacks": one virtual query whose R-row blocks belong to different
+//     queries, so short queries fill the rows a single one would leave as
+//     padding and share every column step; longer queries form stacks of their
+//     own, bucketed by the kernel shape the tuning table picks for them;
+//   * per bucket, one persistent launch of sw_batch<T,R> over its stacks
+//     (blocks walk the stacks in order, groups claim record pairs from one
+//     device counter per stack), plus, when a cut-over is set, a concurrent
 //     launch of single-group blocks for the pairs longer than the cut-over, so
 //     their inherently serial column steps overlap the bulk;
 //   * one 32-bit re-score launch for every flagged (query, record) and one
@@ -36,11 +39,18 @@ struct BatchLaunch {
     const WfKernel* k;
     int grid, threads;
     size_t smem;
-    int qbegin, qcount;        // entries of the qlist
+    int sbegin, scount;        // stacks of this launch
     int pair_begin, pair_count;
     int counter_base;          // first counter of this launch
     bool long_part;            // runs on the side stream
     size_t bnd_group;
+};
+
+// Host image of a batch's stacks (uploaded as one block, see enqueue_batch).
+struct StackPlan {
+    std::vector<uint8_t> codes;           // stack rows
+    std::vector<uint32_t> off, rows, rb_off;
+    std::vector<int32_t> rb_map;
 };
 
 struct BatchGraph {
@@ -50,11 +60,11 @@ struct BatchGraph {
 };
 
 struct sw_batch_state {
-    sw_batch_options opt{8192, 32, 16, 1};
+    sw_batch_options opt{8192, 32, 16, 1, 16, 32, 1024};
     // device
     uint8_t* d_queries = nullptr;
     size_t queries_cap = 0;
-    uint32_t* d_meta = nullptr;      // qoff[nq] | qlen[nq] | qlist[nq] (as uint32)
+    uint8_t* d_meta = nullptr;       // qoff[nq] qlen[nq] | stack codes, off, rows, rb_off, rb_map
     size_t meta_cap = 0;
     int* d_counters = nullptr;       // 2 per query + 1 overflow count
     size_t counters_cap = 0;
@@ -120,24 +130,52 @@ double wall_ms() {
 }
 
 // Enqueues one batch on ctx->stream (and the side stream).  Buffers are sized.
+// Device layout of d_meta (and of the staging area it is copied from):
+//   qoff[nq], qlen[nq]                          uint32
+//   stack_off[ns], stack_rows[ns], rb_off[ns]   uint32
+//   rb_map[...]                                 int32
+//   stack codes                                 uint8
+struct MetaLayout {
+    size_t qoff, qlen, soff, srows, rboff, rbmap, codes, total;
+};
+
+MetaLayout meta_layout(uint32_t nq, const StackPlan& sp) {
+    MetaLayout m;
+    const size_t ns = sp.off.size();
+    m.qoff = 0;
+    m.qlen = m.qoff + 4 * (size_t)nq;
+    m.soff = m.qlen + 4 * (size_t)nq;
+    m.srows = m.soff + 4 * ns;
+    m.rboff = m.srows + 4 * ns;
+    m.rbmap = m.rboff + 4 * ns;
+    m.codes = m.rbmap + 4 * sp.rb_map.size();
+    m.total = (m.codes + sp.codes.size() + 15) / 16 * 16;
+    return m;
+}
+
 sw_status enqueue_batch(sw_ctx* ctx, sw_batch_state* b, uint32_t nq, size_t qbytes,
-                        const std::vector<BatchLaunch>& launches, bool want_scores,
-                        uint32_t* n_launch) {
+                        const MetaLayout& ml, const std::vector<BatchLaunch>& launches,
+                        bool want_scores, uint32_t* n_launch) {
     cudaStream_t st = ctx->stream;
     const int n_rec = (int)ctx->n_records;
     const int k = ctx->params.top_k;
     *n_launch = 0;
-    const size_t meta_bytes = (size_t)3 * nq * sizeof(uint32_t);
     SW_CUDA(ctx, cudaMemcpyAsync(b->d_queries, b->h_stage, qbytes ? qbytes : 1,
                                  cudaMemcpyHostToDevice, st));
-    SW_CUDA(ctx, cudaMemcpyAsync(b->d_meta, b->h_stage + b->stage_cap - meta_bytes, meta_bytes,
+    const size_t meta_at = (b->stage_cap - ml.total) & ~(size_t)15;
+    SW_CUDA(ctx, cudaMemcpyAsync(b->d_meta, b->h_stage + meta_at, ml.total,
                                  cudaMemcpyHostToDevice, st));
-    SW_CUDA(ctx, cudaMemsetAsync(b->d_counters, 0, (2 * (size_t)nq + 1) * sizeof(int), st));
+    const int nst = (int)((ml.rboff - ml.srows) / 4);
+    SW_CUDA(ctx, cudaMemsetAsync(b->d_counters, 0, (2 * (size_t)nst + 1) * sizeof(int), st));
     SW_CUDA(ctx, cudaMemsetAsync(b->d_scores, 0, (size_t)nq * n_rec * sizeof(int), st));
-    const uint32_t* d_qoff = b->d_meta;
-    const uint32_t* d_qlen = b->d_meta + nq;
-    const int* d_qlist = reinterpret_cast<const int*>(b->d_meta + 2 * nq);
-    int* d_ovf_count = b->d_counters + 2 * nq;
+    const uint32_t* d_qoff = reinterpret_cast<const uint32_t*>(b->d_meta + ml.qoff);
+    const uint32_t* d_qlen = reinterpret_cast<const uint32_t*>(b->d_meta + ml.qlen);
+    const uint32_t* d_soff = reinterpret_cast<const uint32_t*>(b->d_meta + ml.soff);
+    const uint32_t* d_srows = reinterpret_cast<const uint32_t*>(b->d_meta + ml.srows);
+    const uint32_t* d_rboff = reinterpret_cast<const uint32_t*>(b->d_meta + ml.rboff);
+    const int* d_rbmap = reinterpret_cast<const int*>(b->d_meta + ml.rbmap);
+    const uint8_t* d_codes = b->d_meta + ml.codes;
+    int* d_ovf_count = b->d_counters + 2 * nst;
     const int ovf_thresh = 32767 - std::max(ctx->max_score, 1) + 1;
     bool forked = false;
     for (const BatchLaunch& L : launches) {
@@ -146,11 +184,12 @@ sw_status enqueue_batch(sw_ctx* ctx, sw_batch_state* b, uint32_t nq, size_t qbyt
         a.pairs = ctx->d_pairs;
         a.pair_begin = L.pair_begin;
         a.pair_count = L.pair_count;
-        a.queries = b->d_queries;
-        a.qoff = d_qoff;
-        a.qlen = d_qlen;
-        a.qlist = d_qlist + L.qbegin;
-        a.nq = L.qcount;
+        a.codes = d_codes;
+        a.stack_off = d_soff + L.sbegin;
+        a.stack_rows = d_srows + L.sbegin;
+        a.rb_map = d_rbmap;
+        a.rb_off = d_rboff + L.sbegin;
+        a.nstacks = L.scount;
         a.counters = b->d_counters + L.counter_base;
         a.mat = ctx->d_mat;
         a.bias2 = (uint32_t)(ctx->params.gap_open + ctx->params.gap_extend);
@@ -165,6 +204,7 @@ sw_status enqueue_batch(sw_ctx* ctx, sw_batch_state* b, uint32_t nq, size_t qbyt
         a.ovf_list = b->d_ovf;
         a.ovf_count = d_ovf_count;
         a.ovf_thresh = ovf_thresh;
+        a.ovf_cap = (int)std::min<size_t>(b->ovf_cap, (size_t)INT32_MAX);
         void* args[] = {&a};
         cudaStream_t ls = st;
         if (L.long_part) {
@@ -198,6 +238,7 @@ sw_status enqueue_batch(sw_ctx* ctx, sw_batch_state* b, uint32_t nq, size_t qbyt
         r.gap_e = ctx->params.gap_extend;
         r.ovf_list = b->d_ovf;
         r.ovf_count = d_ovf_count;
+        r.ovf_cap = (int)std::min<size_t>(b->ovf_cap, (size_t)INT32_MAX);
         r.scratch = ctx->d_rs_scratch;
         r.max_cols = ctx->max_cols;
         r.scores = b->d_scores;
@@ -251,11 +292,12 @@ extern "C" sw_status sw_set_batch_options(sw_ctx* ctx, const sw_batch_options* o
     if (!ctx) return SW_ERR_INVALID;
     if (!ctx->batch) ctx->batch = new sw_batch_state();
     if (opt) {
-        if (opt->cutover < 0 || !find_kernel(opt->long_group_width, opt->long_rows_per_thread))
+        if (opt->cutover < 0 || !find_kernel(opt->long_group_width, opt->long_rows_per_thread) ||
+            !find_kernel(opt->group_width, opt->rows_per_thread) || opt->stack_rows < 0)
             SW_SET(ctx, SW_ERR_INVALID, "bad batch options");
         ctx->batch->opt = *opt;
     } else {
-        ctx->batch->opt = sw_batch_options{8192, 32, 16, 1};
+        ctx->batch->opt = sw_batch_options{8192, 32, 16, 1, 16, 32, 1024};
     }
     for (auto& kv : ctx->batch->graphs) {
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
@@ -292,7 +334,7 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
     if (!ctx->batch) ctx->batch = new sw_batch_state();
     sw_batch_state* b = ctx->batch;
 
-    // ---- plan: queries sorted by length, buckets by tuned shape ----
+    // ---- plan: stacks of queries, buckets by kernel shape ----
     std::vector<uint32_t> qlen(nq), order(nq);
     for (uint32_t i = 0; i < nq; ++i) qlen[i] = (uint32_t)(qoffsets[i + 1] - qoffsets[i]);
     std::iota(order.begin(), order.end(), 0u);
@@ -305,39 +347,105 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
     if (cut > 0)
         while (n_long < ctx->n_pairs && (int)ctx->pair_ncols[n_long] > cut) ++n_long;
     if (n_long == ctx->n_pairs) n_long = 0;     // all long: no split
-    std::vector<BatchLaunch> launches;
-    int counter_base = 0;
-    size_t bnd_long = 0, bnd_bulk = 0;
+
+    // A bucket = one kernel shape and the stacks it runs.  Queries of at least
+    // stack_rows residues: one stack each, shape from the tuning table.  The
+    // shorter ones: packed (first fit, longest first) into stacks of at most
+    // stack_rows rows, each query padded to whole R-row blocks.
+    struct Stack {
+        std::vector<uint32_t> q;        // queries, in row order
+        uint32_t rows = 0;
+    };
+    struct Bucket {
+        int T, R;
+        std::vector<Stack> stacks;
+    };
+    std::vector<Bucket> buckets;
+    const int sT = b->opt.group_width, sR = b->opt.rows_per_thread;
+    const uint32_t cap_rows = (uint32_t)std::max(b->opt.stack_rows, 0);
     uint32_t i0 = 0;
-    while (i0 < nz) {
-        const sw_kernel_config c0 = choose_config(ctx, (int)qlen[order[i0]]);
-        uint32_t i1 = i0 + 1;
-        while (i1 < nz) {
-            const sw_kernel_config c1 = choose_config(ctx, (int)qlen[order[i1]]);
-            if (c1.short_group_width != c0.short_group_width ||
-                c1.short_rows_per_thread != c0.short_rows_per_thread)
-                break;
-            ++i1;
+    while (i0 < nz && qlen[order[i0]] >= cap_rows) {
+        const sw_kernel_config c = choose_config(ctx, (int)qlen[order[i0]]);
+        if (buckets.empty() || buckets.back().T != c.short_group_width ||
+            buckets.back().R != c.short_rows_per_thread || buckets.back().stacks.size() >= 1024)
+            buckets.push_back(Bucket{c.short_group_width, c.short_rows_per_thread, {}});
+        Stack st1;
+        st1.q.push_back(order[i0]);
+        st1.rows = qlen[order[i0]];
+        buckets.back().stacks.push_back(st1);
+        ++i0;
+    }
+    if (i0 < nz) {
+        Bucket bk{sT, sR, {}};
+        for (uint32_t i = i0; i < nz; ++i) {
+            const uint32_t q = order[i];
+            const uint32_t need = (qlen[q] + sR - 1) / sR * sR;
+            bool placed = false;
+            for (Stack& stk : bk.stacks)
+                if (stk.rows + need <= cap_rows) {
+                    stk.q.push_back(q);
+                    stk.rows += need;
+                    placed = true;
+                    break;
+                }
+            if (!placed) {
+                Stack stk;
+                stk.q.push_back(q);
+                stk.rows = need;
+                bk.stacks.push_back(stk);
+            }
         }
-        const int maxq = (int)qlen[order[i0]];
-        const WfKernel* kb = find_kernel(c0.short_group_width, c0.short_rows_per_thread);
-        if (!kb) SW_SET(ctx, SW_ERR_INVALID, "no kernel for the tuned shape");
-        const int occ = shape_occupancy(ctx, *kb, maxq);
+        buckets.push_back(bk);
+    }
+    // host image of every stack: row codes and the (pass, thread) -> query map
+    StackPlan sp;
+    std::vector<BatchLaunch> launches;
+    size_t bnd_long = 0, bnd_bulk = 0;
+    int nst_total = 0;
+    for (const Bucket& bk : buckets) nst_total += (int)bk.stacks.size();
+    int sidx = 0;
+    for (const Bucket& bk : buckets) {
+        const WfKernel* kb = find_kernel(bk.T, bk.R);
+        if (!kb) SW_SET(ctx, SW_ERR_INVALID, "no kernel for shape %dx%d", bk.T, bk.R);
+        uint32_t max_rows = 0;
+        const int s0 = sidx;
+        for (const Stack& stk : bk.stacks) {
+            const uint32_t rows = stk.q.size() == 1 ? qlen[stk.q[0]] : stk.rows;
+            max_rows = std::max(max_rows, rows);
+            sp.off.push_back((uint32_t)sp.codes.size());
+            sp.rows.push_back(rows);
+            sp.rb_off.push_back((uint32_t)sp.rb_map.size());
+            std::vector<int32_t> block_q;           // per R-row block: query | first bit
+            for (const uint32_t q : stk.q) {
+                const uint8_t* src = queries + qoffsets[q];
+                const uint32_t L = qlen[q];
+                const uint32_t padded = stk.q.size() == 1 ? L : (L + bk.R - 1) / bk.R * bk.R;
+                sp.codes.insert(sp.codes.end(), src, src + L);
+                sp.codes.insert(sp.codes.end(), padded - L, (uint8_t)kZeroCode);
+                const uint32_t nblk = (padded + bk.R - 1) / bk.R;
+                for (uint32_t j = 0; j < nblk; ++j)
+                    block_q.push_back((int32_t)q | (j == 0 ? kFirstBit : 0));
+            }
+            const uint32_t P = (rows + bk.T * bk.R - 1) / (bk.T * bk.R);
+            for (uint32_t j = 0; j < P * (uint32_t)bk.T; ++j)
+                sp.rb_map.push_back(j < block_q.size() ? block_q[j] : -1);
+            ++sidx;
+        }
+        const int occ = shape_occupancy(ctx, *kb, (int)max_rows);
         if (occ == 0)
-            SW_SET(ctx, SW_ERR_UNSUPPORTED, "query of %d residues does not fit shape %dx%d", maxq,
+            SW_SET(ctx, SW_ERR_UNSUPPORTED, "stack of %u rows does not fit shape %dx%d", max_rows,
                    kb->T, kb->R);
-        // bulk: pairs [n_long, n_pairs), groups with private boundary rows
-        {
+        {   // bulk: pairs [n_long, n_pairs), groups with private boundary rows
             BatchLaunch L;
             L.k = kb;
             L.threads = kb->block;
             L.grid = occ * ctx->num_sms;
-            L.smem = kb->smem(maxq);
-            L.qbegin = (int)i0;
-            L.qcount = (int)(i1 - i0);
+            L.smem = kb->smem((int)max_rows);
+            L.sbegin = s0;
+            L.scount = sidx - s0;
             L.pair_begin = (int)n_long;
             L.pair_count = (int)(ctx->n_pairs - n_long);
-            L.counter_base = counter_base;
+            L.counter_base = s0;
             L.long_part = false;
             const int cols = n_long > 0 ? ((int)ctx->pair_ncols[n_long] + 7) / 8 * 8 : ctx->max_cols;
             L.bnd_group = 2 * (size_t)cols;
@@ -345,38 +453,46 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
             launches.push_back(L);
         }
         if (n_long > 0) {
-            const WfKernel* kl = find_kernel(b->opt.long_group_width, b->opt.long_rows_per_thread);
-            const int occl = shape_occupancy(ctx, *kl, maxq);
-            if (occl == 0)
-                SW_SET(ctx, SW_ERR_UNSUPPORTED, "query of %d residues does not fit the long shape",
-                       maxq);
+            // long pairs: single-group blocks of the same shape (the stacks'
+            // row maps are laid out for it)
+            const int occl = shape_occupancy(ctx, *kb, (int)max_rows);
             BatchLaunch L;
-            L.k = kl;
-            L.threads = kl->T;
-            L.grid = (int)std::min<int64_t>((int64_t)2 * ctx->num_sms, n_long);
-            L.smem = kl->smem(maxq);
-            L.qbegin = (int)i0;
-            L.qcount = (int)(i1 - i0);
+            L.k = kb;
+            L.threads = kb->T;
+            L.grid = (int)std::min<int64_t>((int64_t)std::max(occl, 1) * 2 * ctx->num_sms, n_long);
+            L.smem = kb->smem((int)max_rows);
+            L.sbegin = s0;
+            L.scount = sidx - s0;
             L.pair_begin = 0;
             L.pair_count = (int)n_long;
-            L.counter_base = counter_base + (int)nq;
+            L.counter_base = nst_total + s0;
             L.long_part = true;
             L.bnd_group = 2 * (size_t)ctx->max_cols;
             bnd_long = std::max(bnd_long, (size_t)L.grid * L.bnd_group);
             launches.push_back(L);
         }
-        counter_base += (int)(i1 - i0);
-        i0 = i1;
     }
-    // counters: bulk i at [i], long i at [nq + i] (i = position in the qlist)
+    // counters: bulk of stack i at [i], long at [nst_total + i], overflow count last
+    const MetaLayout ml = meta_layout(nq, sp);
 
     // ---- buffers (before any capture) ----
     const long long nblk0 = std::max<long long>(1, ((long long)n_rec + kTopkKeys - 1) / kTopkKeys);
     sw_status s;
+    auto drop_graphs = [&]() {
+        for (auto& kv : b->graphs) {      // graphs hold the old pointers
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+            if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+        }
+        b->graphs.clear();
+    };
+    if (std::max<uint64_t>(qbytes, 1) > b->queries_cap || ml.total > b->meta_cap ||
+        2 * (size_t)nst_total + 1 > b->counters_cap)
+        drop_graphs();
     if ((s = grow(ctx, &b->d_queries, b->queries_cap, std::max<uint64_t>(qbytes, 1), "queries")) != SW_OK) return s;
-    if ((s = grow(ctx, &b->d_meta, b->meta_cap, (size_t)3 * nq, "query table")) != SW_OK) return s;
-    if ((s = grow(ctx, &b->d_counters, b->counters_cap, 2 * (size_t)nq + 1, "counters")) != SW_OK) return s;
+    if ((s = grow(ctx, &b->d_meta, b->meta_cap, ml.total, "stack table")) != SW_OK) return s;
+    if ((s = grow(ctx, &b->d_counters, b->counters_cap, 2 * (size_t)nst_total + 1, "counters")) != SW_OK) return s;
     if (nq > b->scores_cap) {
+        drop_graphs();
         dev_free(b->d_scores);
         dev_free(b->d_scores_rec);
         b->scores_cap = 0;
@@ -385,9 +501,15 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
             SW_SET(ctx, SW_ERR_NOMEM, "device allocation failed: batch scores");
         b->scores_cap = nq;
     }
-    if ((s = grow(ctx, &b->d_ovf, b->ovf_cap, (size_t)nq * n_rec + 1, "overflow list")) != SW_OK) return s;
+    // a (query, record) is flagged once per pass its query spans; flags are
+    // rare (scores near 32,767), so twice the records per query is ample and
+    // the kernels drop what would not fit (reported below)
+    const size_t ovf_need = 2 * (size_t)nq * n_rec + 1;
+    if (ovf_need > b->ovf_cap) drop_graphs();
+    if ((s = grow(ctx, &b->d_ovf, b->ovf_cap, ovf_need, "overflow list")) != SW_OK) return s;
     const size_t keys_need = (size_t)nq * nblk0 * kMaxTopK;
     if (keys_need > b->keys_cap) {
+        drop_graphs();
         dev_free(b->d_keys[0]);
         dev_free(b->d_keys[1]);
         b->keys_cap = 0;
@@ -396,38 +518,25 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
             SW_SET(ctx, SW_ERR_NOMEM, "device allocation failed: keys");
         b->keys_cap = keys_need;
     }
-    // boundary rows: long launch in the first half, bulk launches in the second
+    // boundary rows: long launches in the first half, bulk launches in the second
     const size_t bnd_need = 2 * std::max(bnd_long, bnd_bulk) + 2;
     if (bnd_need > b->bnd_cap) {
-        for (auto& kv : b->graphs) {      // graphs hold the old pointer
-            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-            if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
-        }
-        b->graphs.clear();
+        drop_graphs();
         if ((s = grow(ctx, &b->d_bnd, b->bnd_cap, bnd_need, "boundary rows")) != SW_OK) return s;
     }
-    const size_t meta_bytes = (size_t)3 * nq * sizeof(uint32_t);
-    const size_t stage_need = qbytes + meta_bytes + 64;
+    const size_t stage_need = qbytes + ml.total + 64;
     if (stage_need > b->stage_cap) {
-        for (auto& kv : b->graphs) {
-            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-            if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
-        }
-        b->graphs.clear();
+        drop_graphs();
         if (b->h_stage) cudaFreeHost(b->h_stage);
         b->h_stage = nullptr;
         b->stage_cap = 0;
-        const size_t cap = std::max<size_t>(stage_need * 2, 1 << 16);
-        if (cudaMallocHost((void**)&b->h_stage, cap) != cudaSuccess)
+        const size_t capb = std::max<size_t>(stage_need * 2, 1 << 16);
+        if (cudaMallocHost((void**)&b->h_stage, capb) != cudaSuccess)
             SW_SET(ctx, SW_ERR_NOMEM, "pinned staging buffer");
-        b->stage_cap = cap;
+        b->stage_cap = capb;
     }
     if ((size_t)nq * k > b->hkeys_cap) {
-        for (auto& kv : b->graphs) {
-            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-            if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
-        }
-        b->graphs.clear();
+        drop_graphs();
         if (b->h_keys) cudaFreeHost(b->h_keys);
         b->h_keys = nullptr;
         b->hkeys_cap = 0;
@@ -436,13 +545,22 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
         b->hkeys_cap = (size_t)nq * k;
     }
 
-    // ---- stage the inputs: queries, then [qoff | qlen | qlist] at the end ----
+    // ---- stage the inputs: queries at the front, the table at the back ----
     if (qbytes) memcpy(b->h_stage, queries + qoffsets[0], qbytes);
-    uint32_t* meta = reinterpret_cast<uint32_t*>(b->h_stage + b->stage_cap - meta_bytes);
-    for (uint32_t i = 0; i < nq; ++i) {
-        meta[i] = (uint32_t)(qoffsets[i] - qoffsets[0]);
-        meta[nq + i] = qlen[i];
-        meta[2 * nq + i] = order[i];
+    {
+        uint8_t* m = b->h_stage + ((b->stage_cap - ml.total) & ~(size_t)15);
+        uint32_t* qo = reinterpret_cast<uint32_t*>(m + ml.qoff);
+        uint32_t* ql = reinterpret_cast<uint32_t*>(m + ml.qlen);
+        for (uint32_t i = 0; i < nq; ++i) {
+            qo[i] = (uint32_t)(qoffsets[i] - qoffsets[0]);
+            ql[i] = qlen[i];
+        }
+        const size_t ns = sp.off.size();
+        memcpy(m + ml.soff, sp.off.data(), 4 * ns);
+        memcpy(m + ml.srows, sp.rows.data(), 4 * ns);
+        memcpy(m + ml.rboff, sp.rb_off.data(), 4 * ns);
+        memcpy(m + ml.rbmap, sp.rb_map.data(), 4 * sp.rb_map.size());
+        memcpy(m + ml.codes, sp.codes.data(), sp.codes.size());
     }
 
     // ---- run: replay the captured graph for this signature, or capture it ----
@@ -451,6 +569,8 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
     sig.push_back(nq);
     sig.push_back(scores ? 1 : 0);
     sig.push_back((uint64_t)b->opt.cutover);
+    sig.push_back((uint64_t)b->opt.group_width << 32 | (uint32_t)b->opt.rows_per_thread);
+    sig.push_back((uint64_t)b->opt.stack_rows);
     for (uint32_t i = 0; i < nq; ++i) sig.push_back(qlen[i]);
     uint32_t n_launch = 0;
     SW_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));
@@ -459,7 +579,8 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
         if (it == b->graphs.end()) {
             BatchGraph g;
             SW_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
-            sw_status es = enqueue_batch(ctx, b, nq, qbytes, launches, scores != nullptr, &g.launches);
+            sw_status es =
+                enqueue_batch(ctx, b, nq, qbytes, ml, launches, scores != nullptr, &g.launches);
             cudaGraph_t graph = nullptr;
             const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &graph);
             if (es != SW_OK) {
@@ -480,7 +601,7 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
         SW_CUDA(ctx, cudaGraphLaunch(it->second.exec, ctx->stream));
         n_launch = it->second.launches;
     } else {
-        s = enqueue_batch(ctx, b, nq, qbytes, launches, scores != nullptr, &n_launch);
+        s = enqueue_batch(ctx, b, nq, qbytes, ml, launches, scores != nullptr, &n_launch);
         if (s != SW_OK) return s;
     }
     SW_CUDA(ctx, cudaEventRecord(ctx->ev[1], ctx->stream));
@@ -489,6 +610,15 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
                                      cudaMemcpyDeviceToHost, ctx->stream));
     SW_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     SW_CUDA(ctx, cudaGetLastError());
+    {
+        int flagged = 0;
+        SW_CUDA(ctx, cudaMemcpy(&flagged, b->d_counters + 2 * sp.off.size(), sizeof(int),
+                                cudaMemcpyDeviceToHost));
+        if ((size_t)flagged > b->ovf_cap)
+            SW_SET(ctx, SW_ERR_UNSUPPORTED, "%d overflow entries exceed the list (%zu)", flagged,
+                   b->ovf_cap);
+        ctx->stats.rescored = (uint64_t)flagged;
+    }
     for (uint32_t q = 0; q < nq; ++q) {
         uint32_t m = 0;
         for (int i = 0; i < k; ++i) {

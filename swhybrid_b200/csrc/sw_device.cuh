@@ -48,29 +48,34 @@ struct WfArgs {
     int ovf_thresh;             // biased lane value >= this may have wrapped
 };
 
+// Row-block map entry of a stacked batch: the query starts at this block.
+constexpr int kFirstBit = 1 << 30;
+
 // Arguments of the batched first-pass kernel (sw_wavefront.cuh, sw_batch).
 struct BatchArgs {
     const uint4* db;
     const Pair2* pairs;
-    int pair_begin;             // pairs [pair_begin, pair_begin + pair_count) of every query
+    int pair_begin;             // pairs [pair_begin, pair_begin + pair_count) of every stack
     int pair_count;
-    const uint8_t* queries;     // all queries' codes back to back
-    const uint32_t* qoff;       // per query: offset into queries
-    const uint32_t* qlen;       // per query: length
-    const int* qlist;           // the queries of this launch, in order
-    int nq;
-    int* counters;              // one pair counter per entry of qlist (zero before)
+    const uint8_t* codes;       // the stacks' row codes back to back (24 = padding row)
+    const uint32_t* stack_off;  // per stack: offset into codes
+    const uint32_t* stack_rows; // per stack: rows
+    const int* rb_map;          // per stack, per pass and thread: query | first bit, or -1
+    const uint32_t* rb_off;     // per stack: offset into rb_map
+    int nstacks;
+    int* counters;              // one pair counter per stack (zero before)
     const int8_t* mat;
     uint32_t bias2;
     uint32_t neg_e;
     uint32_t one;
     uint2* bnd;                 // per-group boundary rows
     size_t bnd_group;           // entries per group (2 per column of the longest pair)
-    int* scores;                // [query][sorted position]
+    int* scores;                // [query][sorted position], zero before (atomicMax)
     int n_records;
     int* ovf_list;              // query * n_records + position
     int* ovf_count;
     int ovf_thresh;
+    int ovf_cap;                // entries the overflow list holds
 };
 
 __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {

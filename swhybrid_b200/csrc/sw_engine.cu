@@ -613,6 +613,7 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
         r.n_records = (int)ctx->n_records;
         r.ovf_list = ctx->d_ovf;
         r.ovf_count = ctx->d_counters + 2;
+        r.ovf_cap = (int)ctx->n_records + 1;
         r.scratch = ctx->d_rs_scratch;
         r.max_cols = ctx->max_cols;
         r.scores = ctx->d_scores;

@@ -185,12 +185,20 @@ struct RunArgs {
     int* ovf_count;
     int ovf_base;
     int ovf_thresh;             // biased lane value >= this may have wrapped
+    int ovf_cap;                // entries the overflow list holds
+    // stacked queries (batched search): several queries share the rows of one
+    // "stack"; entry pass*T + t holds the query of thread t's rows in that pass
+    // (-1: padding) with bit 30 set when the query starts at the thread's first
+    // row.  Scores then go to scores[query * n_records + position] by atomicMax.
+    const int* rb_map;
 };
+
+
 
 // The group loop: every group of T threads claims pairs from the range and
 // scores them against the query whose profile is in prof.  Returns when the
 // range is exhausted (warp-wide).
-template <int T, int R>
+template <int T, int R, bool STACKED>
 __device__ __forceinline__ void run_pairs(const RunArgs& a, const uint2* prof) {
     static_assert(R % 2 == 0 && R >= 4, "R");
     constexpr int NJ = (R + 7) / 8;    // 8-row profile chunks per thread (last one partial)
@@ -229,10 +237,18 @@ __device__ __forceinline__ void run_pairs(const RunArgs& a, const uint2* prof) {
     uint4 dcur = make_uint4(0u, 0u, 0u, 0u), dnext = dcur;
     uint2 bq0 = make_uint2(Z, Z), bq1 = bq0;
     Pair2 ninfo{0u, 0u};
+    int my_q = 0;           // stacked: this thread's query in the current pass
+    bool my_first = false;  // stacked: that query starts at this thread's first row
 
 #define SWB_START_PASS()                                                   \
     {                                                                      \
         s = 0;                                                             \
+        if (STACKED) {                                                     \
+            const int rb = a.rb_map[pass * T + t];                         \
+            my_first = (rb & kFirstBit) != 0;                              \
+            my_q = (rb < 0) ? -1 : (rb & (kFirstBit - 1));                 \
+            S = Z;                                                         \
+        }                                                                  \
         nsteps = ncols + 2 * T - 1;                                        \
         _Pragma("unroll") for (int k = 0; k < R; ++k) {                    \
             H[k] = Z;                                                      \
@@ -314,6 +330,10 @@ __device__ __forceinline__ void run_pairs(const RunArgs& a, const uint2* prof) {
                     ninfo = a.pairs[a.pair_begin + next];
             }
         }
+        if (STACKED && my_first) {   // a query starts here: nothing flows in from above
+            h_in = Z;
+            f_in = Z;
+        }
         const int ct = s - 2 * t;            // top half's column
         const bool top_valid = ct >= 0 && ct < ncols;
         const bool bot_valid = ct >= 1 && ct <= ncols;
@@ -354,9 +374,41 @@ __device__ __forceinline__ void run_pairs(const RunArgs& a, const uint2* prof) {
         ++s;
         if (!done && s == nsteps) {  // uniform within the group
             __syncwarp(gmask);
+            if (STACKED) {
+                // segmented max over the threads of each query of this pass;
+                // the first thread of a segment adds it to the query's score
+#pragma unroll
+                for (int o = 1; o < T; o <<= 1) {
+                    const uint32_t v = __shfl_down_sync(gmask, S, o, T);
+                    const int qo = __shfl_down_sync(gmask, my_q, o, T);
+                    if (t + o < T && qo == my_q) S = __vimax3_s16x2(S, v, Z);
+                }
+                if (my_q >= 0 && (my_first || t == 0)) {
+                    const int pos = 2 * (a.pair_begin + pair);
+                    const int s0 = lo16(S), s1 = hi16(S);
+                    const int qb = my_q * a.n_records;
+                    atomicMax(a.scores + qb + pos, s0 - bias);
+                    if (s0 >= a.ovf_thresh) {
+                        const int j = atomicAdd(a.ovf_count, 1);
+                        if (j < a.ovf_cap) a.ovf_list[j] = qb + pos;
+                    }
+                    if (pos + 1 < a.n_records) {
+                        atomicMax(a.scores + qb + pos + 1, s1 - bias);
+                        if (s1 >= a.ovf_thresh) {
+                            const int j = atomicAdd(a.ovf_count, 1);
+                            if (j < a.ovf_cap) a.ovf_list[j] = qb + pos + 1;
+                        }
+                    }
+                }
+            }
             if (pass + 1 < P) {
                 ++pass;
                 SWB_START_PASS()
+            } else if (STACKED) {
+                const int v = __shfl_sync(gmask, next, 0, T);
+                off16 = __shfl_sync(gmask, ninfo.off16, 0, T);
+                ncols = (int)__shfl_sync(gmask, ninfo.ncols, 0, T);
+                SWB_TAKE_PAIR(v)
             } else {
 #pragma unroll
                 for (int o = T / 2; o > 0; o >>= 1)
@@ -365,12 +417,16 @@ __device__ __forceinline__ void run_pairs(const RunArgs& a, const uint2* prof) {
                     const int pos = 2 * (a.pair_begin + pair);
                     const int s0 = lo16(S), s1 = hi16(S);
                     a.scores[pos] = s0 - bias;
-                    if (s0 >= a.ovf_thresh)
-                        a.ovf_list[atomicAdd(a.ovf_count, 1)] = a.ovf_base + pos;
+                    if (s0 >= a.ovf_thresh) {
+                        const int j = atomicAdd(a.ovf_count, 1);
+                        if (j < a.ovf_cap) a.ovf_list[j] = a.ovf_base + pos;
+                    }
                     if (pos + 1 < a.n_records) {
                         a.scores[pos + 1] = s1 - bias;
-                        if (s1 >= a.ovf_thresh)
-                            a.ovf_list[atomicAdd(a.ovf_count, 1)] = a.ovf_base + pos + 1;
+                        if (s1 >= a.ovf_thresh) {
+                            const int j = atomicAdd(a.ovf_count, 1);
+                            if (j < a.ovf_cap) a.ovf_list[j] = a.ovf_base + pos + 1;
+                        }
                     }
                 }
                 const int v = __shfl_sync(gmask, next, 0, T);
@@ -409,23 +465,26 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
     r.ovf_count = a.ovf_count;
     r.ovf_base = 0;
     r.ovf_thresh = a.ovf_thresh;
-    run_pairs<T, R>(r, prof);
+    r.ovf_cap = a.n_records + 1;
+    r.rb_map = nullptr;
+    run_pairs<T, R, false>(r, prof);
 }
 
-// Batched search: one persistent launch over a list of queries.  Every block
-// walks the list in order; for each query it rebuilds the profile in shared
-// memory and its groups claim pairs from that query's counter (the device work
-// queue), so the whole grid moves through the queries without a launch per
-// query, and a block only waits for its own groups at a query switch.
+// Batched search: one persistent launch over a list of query stacks (each
+// stack holds one long query or several short ones, aligned to R-row
+// blocks).  Every block walks the stacks in order; for each it rebuilds the
+// profile in shared memory and its groups claim record pairs from that
+// stack's counter (the device work queue), so the whole grid moves through the
+// batch without a launch per query, and a block only waits for its own groups
+// at a stack switch.
 template <int T, int R, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1) sw_batch(const BatchArgs a) {
     extern __shared__ uint2 prof[];
-    for (int i = 0; i < a.nq; ++i) {
-        const int q = a.qlist[i];
-        const int qlen = (int)a.qlen[q];
-        const int P = (qlen + T * R - 1) / (T * R);
+    for (int i = 0; i < a.nstacks; ++i) {
+        const int rows = (int)a.stack_rows[i];
+        const int P = (rows + T * R - 1) / (T * R);
         __syncthreads();        // every group is done with the previous profile
-        build_profile<T, R>(prof, a.queries + a.qoff[q], qlen, a.mat, P);
+        build_profile<T, R>(prof, a.codes + a.stack_off[i], rows, a.mat, P);
         __syncthreads();
         RunArgs r;
         r.db = a.db;
@@ -439,13 +498,15 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_batch(const BatchArgs a) {
         r.one = a.one;
         r.bnd = a.bnd;
         r.bnd_group = a.bnd_group;
-        r.scores = a.scores + (size_t)q * a.n_records;
+        r.scores = a.scores;
         r.n_records = a.n_records;
         r.ovf_list = a.ovf_list;
         r.ovf_count = a.ovf_count;
-        r.ovf_base = q * a.n_records;
+        r.ovf_base = 0;
         r.ovf_thresh = a.ovf_thresh;
-        run_pairs<T, R>(r, prof);
+        r.ovf_cap = a.ovf_cap;
+        r.rb_map = a.rb_map + a.rb_off[i];
+        run_pairs<T, R, true>(r, prof);
     }
 }
 

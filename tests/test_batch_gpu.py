@@ -79,3 +79,25 @@ def test_batch_without_graph_and_empty(ctx):
             np.testing.assert_array_equal(scores[qi], want)
     finally:
         ctx.set_batch_options()
+
+
+def test_many_short_queries_share_stacks(ctx):
+    """Dozens of short queries packed into shared stacks (several per 16x32
+    row block layout), plus planted homologs so some records overflow int16."""
+    rng = np.random.default_rng(43)
+    qs = [synth.residues(rng, int(L)) for L in rng.integers(1, 120, size=40)]
+    db = synth.small_db(14, 2500)
+    db, _ = synth.plant_homologs(rng, db, qs[0], 0.01)
+    ctx.load_db(db.residues, db.offsets)
+    for opts in ({}, {"stack_shape": (16, 8), "stack_rows": 256},
+                 {"stack_shape": (32, 4), "stack_rows": 4096, "cutover": 200}):
+        ctx.set_batch_options(**opts)
+        try:
+            hits, scores = ctx.search_batch(qs, want_scores=True)
+        finally:
+            ctx.set_batch_options()
+        for qi, q in enumerate(qs):
+            want = oracle.search(q, db.residues, db.offsets, M, 12, 2)
+            np.testing.assert_array_equal(scores[qi], want, err_msg=f"{opts} q{qi} len {len(q)}")
+            sc, idx = oracle.topk(want, 10)
+            assert hits[qi] == list(zip(sc.tolist(), idx.tolist()))

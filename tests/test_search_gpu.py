@@ -88,7 +88,7 @@ def test_cutover_split_bit_exact(ctx):
     res, off, queries, gold = load("homolog")
     ctx.load_db(res, off)
     try:
-        for cfg in [(32, 32, 8, 16, 400), (16, 24, 4, 32, 1000), (8, 64, 4, 10, 200), (32, 6, 16, 14, 1500)]:
+        for cfg in [(32, 32, 8, 16, 400), (16, 24, 4, 32, 1000), (8, 64, 4, 10, 200), (32, 6, 16, 12, 1500)]:
             ctx.set_kernel_config(cfg)
             for qi in (0, 1):
                 _, scores = ctx.search(queries[qi], want_scores=True)
