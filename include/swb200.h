@@ -215,8 +215,9 @@ typedef struct sw_batch_options {
     int32_t stack_rows;
 } sw_batch_options;
 
-/* NULL restores the defaults (cut-over 8192, long shape 32x16, graphs on,
- * stacks of up to 1024 rows with shape 16x32). */
+/* NULL restores the defaults (no cut-over, long shape 32x16, graphs on,
+ * stacks of up to 4096 rows with shape 16x64 -- the best measured on B200
+ * for a 64-query batch of lengths 50..5,000 against a 205 M-residue DB). */
 sw_status sw_set_batch_options(struct sw_ctx *ctx, const sw_batch_options *opt);
 
 /* Searches n_queries queries (codes back to back; query_offsets has

@@ -264,8 +264,8 @@ class Context:
         c = sw_kernel_config(*cfg)
         self._check(self.L.sw_set_kernel_config(self.h, ctypes.byref(c)), "sw_set_kernel_config")
 
-    def set_batch_options(self, cutover=8192, long_shape=(32, 16), use_graph=True,
-                          stack_shape=(16, 32), stack_rows=1024):
+    def set_batch_options(self, cutover=0, long_shape=(32, 16), use_graph=True,
+                          stack_shape=(16, 64), stack_rows=4096):
         o = sw_batch_options(cutover, long_shape[0], long_shape[1], 1 if use_graph else 0,
                              stack_shape[0], stack_shape[1], stack_rows)
         self._check(self.L.sw_set_batch_options(self.h, ctypes.byref(o)), "sw_set_batch_options")

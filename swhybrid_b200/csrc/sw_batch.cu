@@ -60,7 +60,7 @@ struct BatchGraph {
 };
 
 struct sw_batch_state {
-    sw_batch_options opt{8192, 32, 16, 1, 16, 32, 1024};
+    sw_batch_options opt{0, 32, 16, 1, 16, 64, 4096};
     // device
     uint8_t* d_queries = nullptr;
     size_t queries_cap = 0;
@@ -297,7 +297,7 @@ extern "C" sw_status sw_set_batch_options(sw_ctx* ctx, const sw_batch_options* o
             SW_SET(ctx, SW_ERR_INVALID, "bad batch options");
         ctx->batch->opt = *opt;
     } else {
-        ctx->batch->opt = sw_batch_options{8192, 32, 16, 1, 16, 32, 1024};
+        ctx->batch->opt = sw_batch_options{0, 32, 16, 1, 16, 64, 4096};
     }
     for (auto& kv : ctx->batch->graphs) {
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);

@@ -543,6 +543,17 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
         SW_CUDA(ctx, cudaEventRecord(ctx->fork_ev, st));
         SW_CUDA(ctx, cudaStreamWaitEvent(ctx->side_stream, ctx->fork_ev, 0));
     }
+    // SMs the long launch reserves; the bulk grid leaves them free so the
+    // long blocks are placed whichever launch the hardware dispatches first
+    int reserved_sms = 0;
+    if (split) {
+        const WfKernel* kl = find_kernel(segs[0].T, segs[0].R);
+        if (kl) {
+            const int64_t gpb = std::max(128, kl->T) / kl->T;
+            reserved_sms = (int)std::max<int64_t>(
+                1, std::min<int64_t>((n_long + gpb - 1) / gpb, ctx->num_sms / 2));
+        }
+    }
     for (int si = 0; si < 2; ++si) {
         const Seg& sg = segs[si];
         if (sg.e <= sg.b) continue;
@@ -583,7 +594,7 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
             SW_CUDA(ctx, cudaLaunchKernel(k->fn, dim3((unsigned)grid), dim3(threads), args,
                                           (size_t)ctx->max_smem, ctx->side_stream));
         } else {
-            int64_t grid = (int64_t)occ * ctx->num_sms;
+            int64_t grid = (int64_t)occ * (ctx->num_sms - reserved_sms);
             const int64_t groups_per_block = k->block / k->T;
             grid = std::min<int64_t>(grid, (groups_needed + groups_per_block - 1) / groups_per_block);
             grid = std::max<int64_t>(grid, 1);

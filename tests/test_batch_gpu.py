@@ -90,7 +90,8 @@ def test_many_short_queries_share_stacks(ctx):
     db, _ = synth.plant_homologs(rng, db, qs[0], 0.01)
     ctx.load_db(db.residues, db.offsets)
     for opts in ({}, {"stack_shape": (16, 8), "stack_rows": 256},
-                 {"stack_shape": (32, 4), "stack_rows": 4096, "cutover": 200}):
+                 {"stack_shape": (32, 4), "stack_rows": 4096, "cutover": 200},
+                 {"stack_shape": (16, 32), "stack_rows": 1024, "cutover": 1000}):
         ctx.set_batch_options(**opts)
         try:
             hits, scores = ctx.search_batch(qs, want_scores=True)
