@@ -116,6 +116,7 @@ __global__ void __launch_bounds__(kTopkThreads) sw_topk_round(const TopkArgs a) 
     __shared__ unsigned long long sk[kTopkKeys];
     const long long base = (long long)blockIdx.x * kTopkKeys;
     const long long y = blockIdx.y;                 // query of a batch
+    const long long ys = (a.rows && !a.keys_in) ? a.rows[y] : y;   // its score row
     for (int i = threadIdx.x; i < kTopkKeys; i += kTopkThreads) {
         const long long g = base + i;
         unsigned long long key = 0ull;
@@ -123,10 +124,10 @@ __global__ void __launch_bounds__(kTopkThreads) sw_topk_round(const TopkArgs a) 
             if (a.keys_in) {
                 key = a.keys_in[y * a.in_stride + g];
             } else {
-                int s = a.scores[y * a.in_stride + g];
+                int s = a.scores[ys * a.in_stride + g];
                 if (a.cap && s > 65535) s = 65535;
                 const uint32_t rec = a.perm[g];
-                if (a.scores_by_record) a.scores_by_record[y * a.rec_stride + rec] = s;
+                if (a.scores_by_record) a.scores_by_record[ys * a.rec_stride + rec] = s;
                 if (s > 0) key = ((unsigned long long)(uint32_t)s << 32) | (0xffffffffu - rec);
             }
         }

@@ -45,6 +45,7 @@ struct TopkArgs {
     long long in_stride;                  // per query (blockIdx.y): scores / keys_in
     long long rec_stride;                 // per query: scores_by_record
     long long out_stride;                 // per query: keys_out
+    const int* rows;                      // optional: round 0 reads score row rows[y]
 };
 
 __global__ void sw_rescore32(const RescoreArgs a);

@@ -205,6 +205,8 @@ sw_status enqueue_batch(sw_ctx* ctx, sw_batch_state* b, uint32_t nq, size_t qbyt
         a.ovf_count = d_ovf_count;
         a.ovf_thresh = ovf_thresh;
         a.ovf_cap = (int)std::min<size_t>(b->ovf_cap, (size_t)INT32_MAX);
+        a.stack_pairs = nullptr;
+        a.pair_ids = nullptr;
         void* args[] = {&a};
         cudaStream_t ls = st;
         if (L.long_part) {
@@ -267,6 +269,7 @@ sw_status enqueue_batch(sw_ctx* ctx, sw_batch_state* b, uint32_t nq, size_t qbyt
         t.in_stride = in_stride;
         t.rec_stride = n_rec;
         t.out_stride = nblk0 * kMaxTopK;
+        t.rows = nullptr;
         void* args[] = {&t};
         SW_CUDA(ctx, cudaLaunchKernel((const void*)sw_topk_round, dim3((unsigned)blocks, nq),
                                       dim3(kTopkThreads), args, 0, st));

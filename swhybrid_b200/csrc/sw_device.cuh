@@ -76,6 +76,8 @@ struct BatchArgs {
     int* ovf_count;
     int ovf_thresh;
     int ovf_cap;                // entries the overflow list holds
+    const int* stack_pairs;     // optional: per stack (pair_begin, pair_count)
+    const uint32_t* pair_ids;   // optional: global pair of each entry of pairs
 };
 
 __device__ __forceinline__ uint32_t prmt(uint32_t a, uint32_t b, uint32_t sel) {

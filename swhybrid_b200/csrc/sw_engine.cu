@@ -653,6 +653,7 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
         t.in_stride = 0;
         t.rec_stride = 0;
         t.out_stride = 0;
+        t.rows = nullptr;
         void* args[] = {&t};
         SW_CUDA(ctx, cudaLaunchKernel((const void*)sw_topk_round, dim3((unsigned)blocks),
                                       dim3(kTopkThreads), args, 0, st));

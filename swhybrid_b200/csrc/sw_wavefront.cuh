@@ -186,6 +186,8 @@ struct RunArgs {
     int ovf_base;
     int ovf_thresh;             // biased lane value >= this may have wrapped
     int ovf_cap;                // entries the overflow list holds
+    const uint32_t* pair_ids;   // optional: global pair of table entry i (a
+                                // permuted table); null = identity
     // stacked queries (batched search): several queries share the rows of one
     // "stack"; entry pass*T + t holds the query of thread t's rows in that pass
     // (-1: padding) with bit 30 set when the query starts at the thread's first
@@ -384,7 +386,9 @@ __device__ __forceinline__ void run_pairs(const RunArgs& a, const uint2* prof) {
                     if (t + o < T && qo == my_q) S = __vimax3_s16x2(S, v, Z);
                 }
                 if (my_q >= 0 && (my_first || t == 0)) {
-                    const int pos = 2 * (a.pair_begin + pair);
+                    const int gp = a.pair_ids ? (int)a.pair_ids[a.pair_begin + pair]
+                                              : a.pair_begin + pair;
+                    const int pos = 2 * gp;
                     const int s0 = lo16(S), s1 = hi16(S);
                     const int qb = my_q * a.n_records;
                     atomicMax(a.scores + qb + pos, s0 - bias);
@@ -466,6 +470,7 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
     r.ovf_base = 0;
     r.ovf_thresh = a.ovf_thresh;
     r.ovf_cap = a.n_records + 1;
+    r.pair_ids = nullptr;
     r.rb_map = nullptr;
     run_pairs<T, R, false>(r, prof);
 }
@@ -489,8 +494,8 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_batch(const BatchArgs a) {
         RunArgs r;
         r.db = a.db;
         r.pairs = a.pairs;
-        r.pair_begin = a.pair_begin;
-        r.pair_count = a.pair_count;
+        r.pair_begin = a.stack_pairs ? a.stack_pairs[2 * i] : a.pair_begin;
+        r.pair_count = a.stack_pairs ? a.stack_pairs[2 * i + 1] : a.pair_count;
         r.counter = a.counters + i;
         r.P = P;
         r.bias2 = a.bias2;
@@ -505,6 +510,7 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_batch(const BatchArgs a) {
         r.ovf_base = 0;
         r.ovf_thresh = a.ovf_thresh;
         r.ovf_cap = a.ovf_cap;
+        r.pair_ids = a.pair_ids;
         r.rb_map = a.rb_map + a.rb_off[i];
         run_pairs<T, R, true>(r, prof);
     }
