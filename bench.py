@@ -67,6 +67,8 @@ def parse():
                     help="force a kernel shape 'T,R,T,R,cutover'")
     ap.add_argument("--no-batched", action="store_true",
                     help="skip the batched (64-query) measurement")
+    ap.add_argument("--serve-requests", type=int, default=96,
+                    help="requests per offered load in the serving leg (0 = skip it)")
     ap.add_argument("--kernel-only", action="store_true",
                     help="time the resident path only (no e2e, probe or CPU baseline)")
     return ap.parse_args()
@@ -249,6 +251,92 @@ def run_reference(args, rank, world):
 
 
 # ---------------------------------------------------------------------------
+def serve_leg(ctx, db, n_req: int, seed: int = 5):
+    """Serving: requests of lengths log-uniform 30..8,000 (seeded) against the
+    resident DB through sw_serve_*.  First the saturating rate (3x the slot
+    count submitted at once), then Poisson arrivals at 25/50/75/100% of it,
+    n_req requests each; every request's top-10 is checked against the plain
+    path for a seeded subset."""
+    from swhybrid_b200 import capi, synth as _synth
+    rng = np.random.default_rng(seed)
+
+    def requests(n):
+        return [_synth.residues(rng, int(L)) for L in _synth.loguniform_lengths(rng, n, 30, 8000)]
+
+    def collect(n, t_limit_s):
+        got = {}
+        t_end = time.time() + t_limit_s
+        while len(got) < n and time.time() < t_end:
+            for r in ctx.serve_poll(256, timeout_ms=100):
+                got[r["id"]] = r
+        return got
+
+    ctx.serve_start()
+    try:
+        slots = int(ctx.serve_stats().slots)
+        # saturating rate: a full queue, throughput from first submit to last completion
+        sat_q = requests(3 * slots)
+        t0 = capi.serve_clock_ms()
+        for i, q in enumerate(sat_q):
+            ctx.serve_submit(i, q)
+        got = collect(len(sat_q), 600)
+        t1 = max(r["done_ms"] for r in got.values())
+        sat_cells = sum(len(q) for q in sat_q) * db.total
+        sat_rate = len(sat_q) / ((t1 - t0) * 1e-3)
+        levels = []
+        check_ids = []
+        base = 1_000_000
+        for frac in (0.25, 0.5, 0.75, 1.0):
+            qs = requests(n_req)
+            arr = _synth.poisson_arrivals(rng, n_req, frac * sat_rate)
+            st0 = ctx.serve_stats()
+            t_start = time.perf_counter()
+            for i, (q, ta) in enumerate(zip(qs, arr)):
+                delay = ta - (time.perf_counter() - t_start)
+                if delay > 0:
+                    time.sleep(delay)
+                ctx.serve_submit(base + i, q)
+            got_l = collect(n_req, 600)
+            st1 = ctx.serve_stats()
+            lat = np.array([r["done_ms"] - r["submit_ms"] for r in got_l.values()])
+            wait = np.array([r["start_ms"] - r["submit_ms"] for r in got_l.values()])
+            first = min(r["submit_ms"] for r in got_l.values())
+            last = max(r["done_ms"] for r in got_l.values())
+            cells = sum(len(q) for q in qs) * db.total
+            levels.append({
+                "offered_fraction": frac,
+                "offered_rate_per_s": round(frac * sat_rate, 3),
+                "requests": n_req, "completed": len(got_l),
+                "ok": int(sum(1 for r in got_l.values() if r["status"] == 0)),
+                "latency_ms_p50": round(float(np.percentile(lat, 50)), 1),
+                "latency_ms_p99": round(float(np.percentile(lat, 99)), 1),
+                "latency_ms_p999": round(float(np.percentile(lat, 99.9)), 1),
+                "queue_wait_ms_p50": round(float(np.percentile(wait, 50)), 1),
+                "gcups": round(cells / ((last - first) * 1e-3) / 1e9, 1),
+                "rounds": int(st1.rounds - st0.rounds),
+                "launches": int(st1.launches - st0.launches),
+            })
+            sel = rng.choice(n_req, size=min(8, n_req), replace=False)
+            check_ids += [(qs[i], got_l.get(base + i)) for i in sel]
+            base += 1_000_000
+        st = ctx.serve_stats()
+    finally:
+        ctx.serve_stop()
+    exact = all(r is not None and r["status"] == 0 and r["hits"] == ctx.search(q)[0]
+                for q, r in check_ids)
+    return {
+        "workload": "requests of lengths log-uniform 30..8,000 (seeded) against the full-size DB; "
+                    "saturating rate from %d requests queued at once, then Poisson arrivals at "
+                    "25/50/75/100%% of it, %d requests per level" % (3 * slots, n_req),
+        "slots": slots, "chunks": int(st.chunks),
+        "saturated": {"requests": len(sat_q), "rate_per_s": round(sat_rate, 3),
+                      "gcups": round(sat_cells / ((t1 - t0) * 1e-3) / 1e9, 1)},
+        "levels": levels,
+        "top10_equal_plain": {"checked": len(check_ids), "all_equal": bool(exact)},
+        "rescored": int(st.rescored),
+    }
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from swhybrid_b200 import capi
@@ -387,6 +475,12 @@ def run_ours(args, rank, world, local_rank):
             "launches_per_batch": b_launches,
         }
 
+    # ---- serving: continuous batching under Poisson arrivals ----
+    served = None
+    if args.workload == "full" and args.serve_requests > 0:
+        ctx.set_stream(None)
+        served = serve_leg(ctx, db, args.serve_requests)
+
     # ---- correctness spot check on the resident DB (rank 0, cheap) ----
     spot = None
     if rank == 0 and args.workload == "small":
@@ -452,6 +546,8 @@ def run_ours(args, rank, world, local_rank):
             line["parity_spot_check"] = spot
         if batched is not None:
             line["batched"] = batched
+        if served is not None:
+            line["served"] = served
     ctx.close()
     return line, db, queries
 

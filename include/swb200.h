@@ -229,6 +229,75 @@ sw_status sw_search_batch(struct sw_ctx *ctx, uint32_t n_queries, const uint8_t 
                           const uint64_t *query_offsets, sw_hit *hits, uint32_t *n_hits,
                           int32_t *scores);
 
+/* ---- serving ------------------------------------------------------------- */
+
+/* The reference serves no requests: src/main.cpp runs one query per process
+ * (Param -> DataPool -> WorkerPool::run).  A serving context keeps the DB
+ * resident and runs a scheduler thread that batches the requests in flight
+ * at every device round (continuous batching): the DB is a ring of `chunks`
+ * chunks of record pairs with the same length mix; every round scores the
+ * next chunk for all requests in flight, short ones packed into shared
+ * stacks as in sw_search_batch; a request joins at the next round boundary
+ * and completes after `chunks` rounds with the same hits sw_search gives.
+ * While serving, sw_db_load, sw_search, sw_search_device, sw_search_batch
+ * and sw_set_stream return SW_ERR_BUSY. */
+typedef struct sw_serve_options {
+    uint32_t max_active;      /* requests in flight on the device (slots) */
+    uint32_t chunks;          /* rounds per request: DB chunks of the ring */
+    uint32_t max_pending;     /* waiting requests before SW_ERR_BUSY (0 = unbounded) */
+    uint64_t memory_budget;   /* device bytes for the slots (0 = half the free memory) */
+    int32_t group_width;      /* kernel shape of the rounds */
+    int32_t rows_per_thread;
+    int32_t stack_rows;       /* requests shorter than this share stacks */
+} sw_serve_options;
+
+/* Defaults: 64 slots, 8 chunks, unbounded queue, half the free memory,
+ * shape 16x64, stacks of 4096 rows. */
+void sw_serve_options_default(sw_serve_options *opt);
+
+typedef struct sw_serve_result {
+    uint64_t request_id;
+    int32_t status;           /* SW_OK, or the error of the round that failed it */
+    uint32_t n_hits;
+    double submit_ms;         /* sw_serve_clock_ms() at submission */
+    double start_ms;          /* ... at admission into a slot */
+    double done_ms;           /* ... when its last round ended */
+} sw_serve_result;
+
+typedef struct sw_serve_stats {
+    uint64_t submitted, admitted, completed, failed;
+    uint64_t rounds, launches, rescored;
+    uint64_t cells;           /* query residues x DB residues of completed requests */
+    double busy_ms;           /* wall time inside device rounds */
+    uint32_t slots, chunks;   /* as sized by sw_serve_start */
+    uint32_t active, pending; /* now */
+} sw_serve_stats;
+
+/* Starts the scheduler thread (opt NULL = defaults).  The slot count is
+ * min(max_active, memory_budget / bytes per request in flight). */
+sw_status sw_serve_start(struct sw_ctx *ctx, const sw_serve_options *opt);
+
+/* Queues a request (codes 0..24, 1..8192 residues).  SW_ERR_BUSY when
+ * max_pending requests already wait; SW_ERR_STATE when not serving. */
+sw_status sw_serve_submit(struct sw_ctx *ctx, uint64_t request_id, const uint8_t *query,
+                          uint32_t qlen);
+
+/* Takes up to max_results completed requests, oldest completion first:
+ * results[i] and hits[i * top_k ..] (score desc, index asc; unused entries
+ * zero).  Waits up to timeout_ms for the first one (0 = no wait, < 0 = no
+ * limit). */
+sw_status sw_serve_poll(struct sw_ctx *ctx, uint32_t max_results, sw_serve_result *results,
+                        sw_hit *hits, uint32_t *n_results, int32_t timeout_ms);
+
+sw_status sw_serve_get_stats(struct sw_ctx *ctx, sw_serve_stats *out);
+
+/* The clock of the result timestamps (steady, milliseconds). */
+double sw_serve_clock_ms(void);
+
+/* Drops waiting requests, lets the ones in flight finish (their results stay
+ * unread), joins the scheduler and frees the serving memory. */
+sw_status sw_serve_stop(struct sw_ctx *ctx);
+
 /* ---- scoring without allocation ------------------------------------------ */
 
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc

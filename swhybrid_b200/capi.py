@@ -29,7 +29,8 @@ EXPORTS = [
     "sw_search_device", "sw_set_kernel_config", "sw_get_kernel_config",
     "sw_get_run_stats", "sw_set_stream", "sw_sync", "sw_reset_totals", "sw_get_totals",
     "sw_set_tuning", "sw_score_noalloc", "sw_get_shapes", "sw_set_batch_options",
-    "sw_search_batch",
+    "sw_search_batch", "sw_serve_options_default", "sw_serve_start", "sw_serve_submit",
+    "sw_serve_poll", "sw_serve_get_stats", "sw_serve_clock_ms", "sw_serve_stop",
 ]
 
 
@@ -65,6 +66,29 @@ class sw_batch_options(ctypes.Structure):
                 ("long_rows_per_thread", ctypes.c_int32), ("use_graph", ctypes.c_int32),
                 ("group_width", ctypes.c_int32), ("rows_per_thread", ctypes.c_int32),
                 ("stack_rows", ctypes.c_int32)]
+
+
+class sw_serve_options(ctypes.Structure):
+    _fields_ = [("max_active", ctypes.c_uint32), ("chunks", ctypes.c_uint32),
+                ("max_pending", ctypes.c_uint32), ("memory_budget", ctypes.c_uint64),
+                ("group_width", ctypes.c_int32), ("rows_per_thread", ctypes.c_int32),
+                ("stack_rows", ctypes.c_int32)]
+
+
+class sw_serve_result(ctypes.Structure):
+    _fields_ = [("request_id", ctypes.c_uint64), ("status", ctypes.c_int32),
+                ("n_hits", ctypes.c_uint32), ("submit_ms", ctypes.c_double),
+                ("start_ms", ctypes.c_double), ("done_ms", ctypes.c_double)]
+
+
+class sw_serve_stats(ctypes.Structure):
+    _fields_ = [("submitted", ctypes.c_uint64), ("admitted", ctypes.c_uint64),
+                ("completed", ctypes.c_uint64), ("failed", ctypes.c_uint64),
+                ("rounds", ctypes.c_uint64), ("launches", ctypes.c_uint64),
+                ("rescored", ctypes.c_uint64), ("cells", ctypes.c_uint64),
+                ("busy_ms", ctypes.c_double), ("slots", ctypes.c_uint32),
+                ("chunks", ctypes.c_uint32), ("active", ctypes.c_uint32),
+                ("pending", ctypes.c_uint32)]
 
 
 class sw_tuning_entry(ctypes.Structure):
@@ -152,8 +176,29 @@ def load(path: str = LIB_PATH):
     L.sw_score_noalloc.argtypes = [ctypes.c_int, ctypes.POINTER(sw_params), ctypes.c_void_p,
                                    ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                    ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]
+    L.sw_serve_options_default.restype = None
+    L.sw_serve_options_default.argtypes = [ctypes.POINTER(sw_serve_options)]
+    L.sw_serve_start.restype = ctypes.c_int
+    L.sw_serve_start.argtypes = [P, ctypes.POINTER(sw_serve_options)]
+    L.sw_serve_submit.restype = ctypes.c_int
+    L.sw_serve_submit.argtypes = [P, ctypes.c_uint64, P, ctypes.c_uint32]
+    L.sw_serve_poll.restype = ctypes.c_int
+    L.sw_serve_poll.argtypes = [P, ctypes.c_uint32, ctypes.POINTER(sw_serve_result),
+                                ctypes.POINTER(sw_hit), ctypes.POINTER(ctypes.c_uint32),
+                                ctypes.c_int32]
+    L.sw_serve_get_stats.restype = ctypes.c_int
+    L.sw_serve_get_stats.argtypes = [P, ctypes.POINTER(sw_serve_stats)]
+    L.sw_serve_clock_ms.restype = ctypes.c_double
+    L.sw_serve_clock_ms.argtypes = []
+    L.sw_serve_stop.restype = ctypes.c_int
+    L.sw_serve_stop.argtypes = [P]
     _lib = L
     return L
+
+
+def serve_clock_ms() -> float:
+    """The clock of served requests' timestamps (steady, milliseconds)."""
+    return load().sw_serve_clock_ms()
 
 
 def default_params(gap_open=10, gap_extend=2, top_k=10, matrix=None,
@@ -317,6 +362,60 @@ class Context:
         t = sw_totals()
         self._check(self.L.sw_get_totals(self.h, ctypes.byref(t)), "sw_get_totals")
         return t
+
+    # ---- serving ----------------------------------------------------------
+    def serve_start(self, max_active=None, chunks=None, max_pending=None, memory_budget=None,
+                    shape=None, stack_rows=None):
+        o = sw_serve_options()
+        self.L.sw_serve_options_default(ctypes.byref(o))
+        if max_active is not None:
+            o.max_active = max_active
+        if chunks is not None:
+            o.chunks = chunks
+        if max_pending is not None:
+            o.max_pending = max_pending
+        if memory_budget is not None:
+            o.memory_budget = memory_budget
+        if shape is not None:
+            o.group_width, o.rows_per_thread = shape
+        if stack_rows is not None:
+            o.stack_rows = stack_rows
+        self._check(self.L.sw_serve_start(self.h, ctypes.byref(o)), "sw_serve_start")
+
+    def serve_submit(self, request_id: int, query: np.ndarray) -> int:
+        """Queues a request; returns SW_OK (0) or SW_ERR_BUSY (7) when the
+        waiting queue is full; raises on any other status."""
+        q = np.ascontiguousarray(query, dtype=np.uint8)
+        st = self.L.sw_serve_submit(self.h, request_id, _ptr(q) if q.size else None, q.size)
+        if st not in (0, 7):
+            raise SwError(st, f"sw_serve_submit: {STATUS.get(st, st)}")
+        return st
+
+    def serve_poll(self, max_results: int = 64, timeout_ms: int = 0) -> list:
+        """Completed requests: dicts with id, status, hits [(score, index)],
+        submit_ms, start_ms, done_ms."""
+        k = self.params.top_k
+        res = (sw_serve_result * max(max_results, 1))()
+        hits = (sw_hit * max(max_results * k, 1))()
+        n = ctypes.c_uint32(0)
+        self._check(self.L.sw_serve_poll(self.h, max_results, res, hits, ctypes.byref(n),
+                                         timeout_ms), "sw_serve_poll")
+        out = []
+        for i in range(n.value):
+            r = res[i]
+            out.append(dict(id=r.request_id, status=r.status,
+                            hits=[(hits[i * k + j].score, hits[i * k + j].index)
+                                  for j in range(r.n_hits)],
+                            submit_ms=r.submit_ms, start_ms=r.start_ms, done_ms=r.done_ms))
+        return out
+
+    def serve_stats(self) -> sw_serve_stats:
+        s = sw_serve_stats()
+        self._check(self.L.sw_serve_get_stats(self.h, ctypes.byref(s)), "sw_serve_get_stats")
+        return s
+
+    def serve_stop(self):
+        self._check(self.L.sw_serve_stop(self.h), "sw_serve_stop")
 
     def run_stats(self) -> sw_run_stats:
         s = sw_run_stats()

@@ -205,7 +205,6 @@ sw_status enqueue_batch(sw_ctx* ctx, sw_batch_state* b, uint32_t nq, size_t qbyt
         a.ovf_count = d_ovf_count;
         a.ovf_thresh = ovf_thresh;
         a.ovf_cap = (int)std::min<size_t>(b->ovf_cap, (size_t)INT32_MAX);
-        a.stack_pairs = nullptr;
         a.pair_ids = nullptr;
         void* args[] = {&a};
         cudaStream_t ls = st;
@@ -314,6 +313,7 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
                                      const uint64_t* qoffsets, sw_hit* hits, uint32_t* n_hits,
                                      int32_t* scores) {
     if (!ctx) return SW_ERR_INVALID;
+    if (ctx->serve) return SW_ERR_BUSY;   // the serving loop owns the stream
     if (!ctx->db_loaded) SW_SET(ctx, SW_ERR_STATE, "no DB loaded (call sw_db_load first)");
     if (nq == 0) return SW_OK;
     if (!qoffsets || !hits || !n_hits) SW_SET(ctx, SW_ERR_INVALID, "null argument");

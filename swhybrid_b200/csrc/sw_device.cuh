@@ -76,7 +76,6 @@ struct BatchArgs {
     int* ovf_count;
     int ovf_thresh;
     int ovf_cap;                // entries the overflow list holds
-    const int* stack_pairs;     // optional: per stack (pair_begin, pair_count)
     const uint32_t* pair_ids;   // optional: global pair of each entry of pairs
 };
 

@@ -237,6 +237,7 @@ static void free_db(sw_ctx* ctx) {
 extern "C" sw_status sw_ctx_destroy(sw_ctx* ctx) {
     if (!ctx) return SW_ERR_INVALID;
     cudaSetDevice(ctx->device);
+    serve_teardown(ctx);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     if (ctx->own_stream) cudaStreamSynchronize(ctx->own_stream);
     if (ctx->side_stream) cudaStreamSynchronize(ctx->side_stream);
@@ -266,6 +267,7 @@ extern "C" sw_status sw_ctx_destroy(sw_ctx* ctx) {
 extern "C" sw_status sw_db_load(sw_ctx* ctx, const uint8_t* residues, const uint64_t* offsets,
                                 uint64_t n) {
     if (!ctx) return SW_ERR_INVALID;
+    if (ctx->serve) return SW_ERR_BUSY;   // the serving loop owns the stream and the DB
     if (!offsets || (n && !residues && offsets[n] != offsets[0]))
         SW_SET(ctx, SW_ERR_INVALID, "null residues/offsets");
     if (n >= (1ull << 31)) SW_SET(ctx, SW_ERR_UNSUPPORTED, "too many records (%llu)",
@@ -715,6 +717,7 @@ sw_status ensure_query_buffers(sw_ctx* ctx, size_t qlen) {
 extern "C" sw_status sw_search(sw_ctx* ctx, const uint8_t* query, uint32_t qlen, sw_hit* hits,
                                uint32_t* n_hits, int32_t* scores) {
     if (!ctx) return SW_ERR_INVALID;
+    if (ctx->serve) return SW_ERR_BUSY;   // the serving loop owns the stream and the DB
     if (!ctx->db_loaded) SW_SET(ctx, SW_ERR_STATE, "no DB loaded (call sw_db_load first)");
     if ((qlen && !query) || (!hits && ctx->params.top_k > 0) || !n_hits)
         SW_SET(ctx, SW_ERR_INVALID, "null argument");
@@ -776,6 +779,7 @@ extern "C" sw_status sw_search(sw_ctx* ctx, const uint8_t* query, uint32_t qlen,
 extern "C" sw_status sw_search_device(sw_ctx* ctx, const uint8_t* d_query, uint32_t qlen,
                                       int32_t* d_scores) {
     if (!ctx) return SW_ERR_INVALID;
+    if (ctx->serve) return SW_ERR_BUSY;   // the serving loop owns the stream and the DB
     if (!ctx->db_loaded) SW_SET(ctx, SW_ERR_STATE, "no DB loaded (call sw_db_load first)");
     if (!d_query || qlen == 0) SW_SET(ctx, SW_ERR_INVALID, "empty query");
     SW_CUDA(ctx, cudaSetDevice(ctx->device));
@@ -792,6 +796,7 @@ extern "C" sw_status sw_search_device(sw_ctx* ctx, const uint8_t* d_query, uint3
 
 extern "C" sw_status sw_set_stream(sw_ctx* ctx, void* cuda_stream) {
     if (!ctx) return SW_ERR_INVALID;
+    if (ctx->serve) return SW_ERR_BUSY;   // the serving loop owns the stream and the DB
     SW_CUDA(ctx, cudaSetDevice(ctx->device));
     sw_status st = drain(ctx, nullptr, nullptr);
     if (st != SW_OK) return st;

@@ -40,6 +40,7 @@ inline void dev_free(T*& p) {
 }
 
 struct sw_batch_state;   // batched search buffers and captured graphs (sw_batch.cu)
+struct sw_serve_state;   // serving loop: slots, ring of DB chunks, scheduler (sw_serve.cu)
 
 struct sw_ctx {
     int device = 0;
@@ -85,6 +86,7 @@ struct sw_ctx {
     uint2* d_rs_scratch = nullptr;     // 32-bit re-score: one boundary row per warp
     int max_cols = 0;                  // longest pair, padded to 8 columns
     sw_batch_state* batch = nullptr;
+    sw_serve_state* serve = nullptr;   // non-null between sw_serve_start and sw_serve_stop
 
     // per-query buffers
     size_t query_cap = 0;
@@ -107,4 +109,5 @@ sw_kernel_config choose_config(sw_ctx* ctx, int qlen);
 sw_status take_marks(sw_ctx* ctx, sw_ctx::Marks* m);
 sw_status drain(sw_ctx* ctx, float* last_ms, float* last_fp_ms);
 void free_batch(sw_ctx* ctx);
+void serve_teardown(sw_ctx* ctx);
 }  // namespace swb

@@ -1,0 +1,633 @@
+// sw_serve.cu -- serving: a request loop with continuous batching on the
+// device.
+//
+// The reference has no serving mode (one query per process run,
+// src/main.cpp).  Here a scheduler thread owns the context between
+// sw_serve_start and sw_serve_stop:
+//   * the DB's record pairs are dealt round-robin (longest first) into
+//     `chunks` chunks with the same length mix, and the chunks form a ring;
+//   * a device round scores the next chunk of the ring for every request in
+//     flight: one persistent launch of the stacked batched kernel (sw_batch)
+//     over all of them (short requests share R-row blocks of a stack, long
+//     ones get stacks of their own), one 32-bit re-score launch for the
+//     round's flagged (request, record) entries and, for the requests that
+//     have now seen every chunk, one top-k round sequence and the download
+//     of their keys;
+//   * a request joins the ring at whatever chunk is next and completes after
+//     `chunks` rounds, so a request that arrives while a round runs waits at
+//     most that round before its work shares the device with everything
+//     already in flight (iteration-level batching);
+//   * admission happens at every round boundary into free slots.  A slot is
+//     the device memory of one request in flight (its score row); the slot
+//     count is bounded by max_active and by a device-memory budget, and the
+//     waiting queue by max_pending (SW_ERR_BUSY beyond it).
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/swb200.h"
+#include "sw_aux.h"
+#include "sw_device.cuh"
+#include "sw_engine.h"
+#include "sw_registry.h"
+
+using namespace swb;
+
+namespace {
+
+constexpr uint32_t kServeMaxQuery = 8192;     // residues per request
+
+double now_ms() {
+    return std::chrono::duration<double, std::milli>(
+               std::chrono::steady_clock::now().time_since_epoch())
+        .count();
+}
+
+struct Request {
+    uint64_t id = 0;
+    std::vector<uint8_t> query;
+    double submit_ms = 0, start_ms = 0, done_ms = 0;
+    sw_status status = SW_OK;
+    std::vector<sw_hit> hits;
+};
+
+struct Slot {
+    bool used = false;
+    bool fresh = false;     // admitted at this round boundary: score row to clear
+    int done_chunks = 0;    // chunks scored so far
+    Request req;
+};
+
+}  // namespace
+
+struct sw_serve_state {
+    sw_serve_options opt{};
+    const WfKernel* k = nullptr;
+    int n_slots = 0;
+    int n_chunks = 1;
+    int occ_max = 0;                      // most blocks per SM any stack height gives
+    std::vector<int> chunk_begin;         // n_chunks + 1 entries into d_pairs
+    Pair2* d_pairs = nullptr;             // pair table, chunk after chunk
+    uint32_t* d_pair_ids = nullptr;       // global pair index of each entry
+    int* d_scores = nullptr;              // [slot][sorted position]
+    uint8_t* d_meta = nullptr;            // per-round tables (layout in run_round)
+    size_t meta_cap = 0;
+    int* d_counters = nullptr;            // one per stack, overflow count last
+    int* d_ovf = nullptr;
+    size_t ovf_cap = 0;
+    uint2* d_bnd = nullptr;
+    size_t bnd_group = 0;
+    unsigned long long* d_keys[2] = {nullptr, nullptr};
+    uint8_t* h_stage = nullptr;           // pinned: per-round tables
+    size_t stage_cap = 0;
+    unsigned long long* h_keys = nullptr; // pinned: n_slots * top_k
+    int cursor = 0;                       // next chunk of the ring
+    std::vector<Slot> slots;
+    std::deque<Request> pending, done;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    bool stopping = false;
+    std::thread th;
+    sw_serve_stats stats{};
+};
+
+namespace {
+
+void serve_free(sw_serve_state* s) {
+    dev_free(s->d_pairs);
+    dev_free(s->d_pair_ids);
+    dev_free(s->d_scores);
+    dev_free(s->d_meta);
+    dev_free(s->d_counters);
+    dev_free(s->d_ovf);
+    dev_free(s->d_bnd);
+    dev_free(s->d_keys[0]);
+    dev_free(s->d_keys[1]);
+    if (s->h_stage) cudaFreeHost(s->h_stage);
+    if (s->h_keys) cudaFreeHost(s->h_keys);
+    s->h_stage = nullptr;
+    s->h_keys = nullptr;
+}
+
+// One device round: chunk `chunk` for every active slot.  `finishing` gets
+// the slots whose cycle ends with this round; their keys land in h_keys in
+// that order.  Runs on the scheduler thread only.
+sw_status run_round(sw_ctx* ctx, sw_serve_state* s, int chunk, std::vector<int>& finishing,
+                    uint32_t* launches, uint64_t* rescored) {
+    cudaStream_t st = ctx->stream;
+    const int n_rec = (int)ctx->n_records;
+    const int T = s->k->T, R = s->k->R;
+    const uint32_t cap_rows = (uint32_t)std::max<int32_t>(s->opt.stack_rows, R);
+    *launches = 0;
+    *rescored = 0;
+    std::vector<int> active;
+    finishing.clear();
+    for (int i = 0; i < s->n_slots; ++i)
+        if (s->slots[i].used) {
+            active.push_back(i);
+            if (s->slots[i].done_chunks + 1 == s->n_chunks) finishing.push_back(i);
+        }
+    // stacks: first fit, longest first; requests of at least cap_rows rows
+    // get a stack each
+    std::stable_sort(active.begin(), active.end(), [&](int a, int b) {
+        return s->slots[a].req.query.size() > s->slots[b].req.query.size();
+    });
+    struct Stack {
+        std::vector<int> slots;
+        uint32_t rows = 0;
+    };
+    std::vector<Stack> stacks;
+    for (int sl : active) {
+        const uint32_t L = (uint32_t)s->slots[sl].req.query.size();
+        const uint32_t need = (L + R - 1) / R * R;
+        bool placed = false;
+        if (L < cap_rows)
+            for (Stack& stk : stacks)
+                if (stk.rows + need <= cap_rows) {
+                    stk.slots.push_back(sl);
+                    stk.rows += need;
+                    placed = true;
+                    break;
+                }
+        if (!placed) {
+            Stack stk;
+            stk.slots.push_back(sl);
+            stk.rows = need;
+            stacks.push_back(stk);
+        }
+    }
+    // Device tables of this round, one upload:
+    //   qoff[n_slots], qlen[n_slots]                uint32 (re-score: slot -> its codes)
+    //   stack_off[ns], stack_rows[ns], rb_off[ns]   uint32
+    //   rb_map[...]                                 int32
+    //   rows[finishing]                             int32 (top-k score rows)
+    //   codes, every stack's rows back to back      uint8
+    const size_t ns = stacks.size();
+    std::vector<uint32_t> qoff((size_t)s->n_slots, 0), qlen((size_t)s->n_slots, 0), soff, srows, rboff;
+    std::vector<int32_t> rbmap;
+    std::vector<uint8_t> codes;
+    uint32_t max_rows = 0;
+    for (const Stack& stk : stacks) {
+        soff.push_back((uint32_t)codes.size());
+        rboff.push_back((uint32_t)rbmap.size());
+        std::vector<int32_t> block_q;          // per R-row block: slot | first bit
+        for (int sl : stk.slots) {
+            const std::vector<uint8_t>& q = s->slots[sl].req.query;
+            const uint32_t L = (uint32_t)q.size();
+            const uint32_t padded = (L + R - 1) / R * R;
+            qoff[sl] = (uint32_t)codes.size();
+            qlen[sl] = L;
+            codes.insert(codes.end(), q.begin(), q.end());
+            codes.insert(codes.end(), padded - L, (uint8_t)kZeroCode);
+            for (uint32_t j = 0; j < padded / R; ++j)
+                block_q.push_back((int32_t)sl | (j == 0 ? kFirstBit : 0));
+        }
+        srows.push_back(stk.rows);
+        max_rows = std::max(max_rows, stk.rows);
+        const uint32_t P = (stk.rows + T * R - 1) / (T * R);
+        for (uint32_t j = 0; j < P * (uint32_t)T; ++j)
+            rbmap.push_back(j < block_q.size() ? block_q[j] : -1);
+    }
+    const size_t o_qoff = 0, o_qlen = 4 * (size_t)s->n_slots, o_soff = 8 * (size_t)s->n_slots;
+    const size_t o_srows = o_soff + 4 * ns, o_rboff = o_srows + 4 * ns, o_rbmap = o_rboff + 4 * ns;
+    const size_t o_rows = o_rbmap + 4 * rbmap.size();
+    const size_t o_codes = o_rows + 4 * finishing.size();
+    const size_t total = (o_codes + codes.size() + 15) / 16 * 16;
+    if (total > s->meta_cap) {
+        dev_free(s->d_meta);
+        s->meta_cap = 0;
+        if (dev_alloc(&s->d_meta, total * 2) != cudaSuccess)
+            SW_SET(ctx, SW_ERR_NOMEM, "device allocation failed: serving tables");
+        s->meta_cap = total * 2;
+    }
+    if (total > s->stage_cap) {
+        // the previous round's upload has completed (every round ends synchronised)
+        if (s->h_stage) cudaFreeHost(s->h_stage);
+        s->h_stage = nullptr;
+        s->stage_cap = 0;
+        if (cudaMallocHost((void**)&s->h_stage, total * 2) != cudaSuccess)
+            SW_SET(ctx, SW_ERR_NOMEM, "pinned allocation failed: serving tables");
+        s->stage_cap = total * 2;
+    }
+    uint8_t* m = s->h_stage;
+    memcpy(m + o_qoff, qoff.data(), 4 * qoff.size());
+    memcpy(m + o_qlen, qlen.data(), 4 * qlen.size());
+    if (ns) {
+        memcpy(m + o_soff, soff.data(), 4 * ns);
+        memcpy(m + o_srows, srows.data(), 4 * ns);
+        memcpy(m + o_rboff, rboff.data(), 4 * ns);
+        memcpy(m + o_rbmap, rbmap.data(), 4 * rbmap.size());
+    }
+    if (!finishing.empty()) memcpy(m + o_rows, finishing.data(), 4 * finishing.size());
+    if (!codes.empty()) memcpy(m + o_codes, codes.data(), codes.size());
+    SW_CUDA(ctx, cudaMemcpyAsync(s->d_meta, m, total, cudaMemcpyHostToDevice, st));
+    // score rows of requests admitted at this boundary start at zero (atomicMax)
+    for (int sl : active)
+        if (s->slots[sl].fresh)
+            SW_CUDA(ctx, cudaMemsetAsync(s->d_scores + (size_t)sl * n_rec, 0,
+                                         (size_t)n_rec * sizeof(int), st));
+    SW_CUDA(ctx, cudaMemsetAsync(s->d_counters, 0, (ns + 1) * sizeof(int), st));
+    const int occ = std::min(shape_occupancy(ctx, *s->k, (int)max_rows), s->occ_max);
+    if (occ <= 0)
+        SW_SET(ctx, SW_ERR_UNSUPPORTED, "a stack of %u rows does not fit shape %dx%d", max_rows,
+               T, R);
+    int* d_ovf_count = s->d_counters + ns;
+    {
+        BatchArgs a;
+        a.db = ctx->d_db;
+        a.pairs = s->d_pairs;
+        a.pair_begin = s->chunk_begin[chunk];
+        a.pair_count = s->chunk_begin[chunk + 1] - s->chunk_begin[chunk];
+        a.codes = s->d_meta + o_codes;
+        a.stack_off = reinterpret_cast<const uint32_t*>(s->d_meta + o_soff);
+        a.stack_rows = reinterpret_cast<const uint32_t*>(s->d_meta + o_srows);
+        a.rb_map = reinterpret_cast<const int*>(s->d_meta + o_rbmap);
+        a.rb_off = reinterpret_cast<const uint32_t*>(s->d_meta + o_rboff);
+        a.nstacks = (int)ns;
+        a.counters = s->d_counters;
+        a.mat = ctx->d_mat;
+        a.bias2 = (uint32_t)(ctx->params.gap_open + ctx->params.gap_extend);
+        a.bias2 |= a.bias2 << 16;
+        a.neg_e = (uint32_t)(uint16_t)(int16_t)(-ctx->params.gap_extend);
+        a.neg_e |= a.neg_e << 16;
+        a.one = 1u;
+        a.bnd = s->d_bnd;
+        a.bnd_group = s->bnd_group;
+        a.scores = s->d_scores;
+        a.n_records = n_rec;
+        a.ovf_list = s->d_ovf;
+        a.ovf_count = d_ovf_count;
+        a.ovf_thresh = 32767 - std::max(ctx->max_score, 1) + 1;
+        a.ovf_cap = (int)std::min<size_t>(s->ovf_cap, (size_t)INT32_MAX);
+        a.pair_ids = s->d_pair_ids;
+        void* args[] = {&a};
+        if (a.pair_count > 0) {
+            SW_CUDA(ctx, cudaLaunchKernel(s->k->batch_fn, dim3((unsigned)(occ * ctx->num_sms)),
+                                          dim3(s->k->block), args, s->k->smem((int)max_rows), st));
+            ++*launches;
+        }
+    }
+    {
+        RescoreArgs r;
+        r.db = ctx->d_db;
+        r.pairs = ctx->d_pairs;
+        r.query = nullptr;
+        r.qlen = 0;
+        r.queries = s->d_meta + o_codes;
+        r.qoff = reinterpret_cast<const uint32_t*>(s->d_meta + o_qoff);
+        r.qlens = reinterpret_cast<const uint32_t*>(s->d_meta + o_qlen);
+        r.n_records = n_rec;
+        r.mat = ctx->d_mat;
+        r.gap_oe = ctx->params.gap_open + ctx->params.gap_extend;
+        r.gap_e = ctx->params.gap_extend;
+        r.ovf_list = s->d_ovf;
+        r.ovf_count = d_ovf_count;
+        r.ovf_cap = (int)std::min<size_t>(s->ovf_cap, (size_t)INT32_MAX);
+        r.scratch = ctx->d_rs_scratch;
+        r.max_cols = ctx->max_cols;
+        r.scores = s->d_scores;
+        void* args[] = {&r};
+        SW_CUDA(ctx, cudaLaunchKernel((const void*)sw_rescore32, dim3(kRescoreBlocks), dim3(64),
+                                      args, 0, st));
+        ++*launches;
+    }
+    if (!finishing.empty()) {
+        const int k = ctx->params.top_k;
+        const long long nblk0 = std::max<long long>(1, ((long long)n_rec + kTopkKeys - 1) / kTopkKeys);
+        long long n = n_rec, in_stride = n_rec;
+        int buf = 0;
+        const unsigned long long* keys_in = nullptr;
+        bool first = true;
+        while (true) {
+            const long long blocks = std::max<long long>(1, (n + kTopkKeys - 1) / kTopkKeys);
+            TopkArgs t;
+            t.scores = s->d_scores;
+            t.perm = ctx->d_perm;
+            t.keys_in = first ? nullptr : keys_in;
+            t.n = n;
+            t.k = k;
+            t.cap = (ctx->params.flags & SW_FLAG_REFERENCE_CAP) ? 1 : 0;
+            t.scores_by_record = nullptr;
+            t.keys_out = s->d_keys[buf];
+            t.in_stride = in_stride;
+            t.rec_stride = 0;
+            t.out_stride = nblk0 * kMaxTopK;
+            t.rows = reinterpret_cast<const int*>(s->d_meta + o_rows);
+            void* args[] = {&t};
+            SW_CUDA(ctx, cudaLaunchKernel((const void*)sw_topk_round,
+                                          dim3((unsigned)blocks, (unsigned)finishing.size()),
+                                          dim3(kTopkThreads), args, 0, st));
+            ++*launches;
+            keys_in = s->d_keys[buf];
+            in_stride = nblk0 * kMaxTopK;
+            buf ^= 1;
+            first = false;
+            if (blocks == 1) break;
+            n = blocks * (long long)k;
+        }
+        SW_CUDA(ctx, cudaMemcpy2DAsync(s->h_keys, (size_t)k * sizeof(unsigned long long), keys_in,
+                                       (size_t)(nblk0 * kMaxTopK) * sizeof(unsigned long long),
+                                       (size_t)k * sizeof(unsigned long long), finishing.size(),
+                                       cudaMemcpyDeviceToHost, st));
+    }
+    SW_CUDA(ctx, cudaStreamSynchronize(st));
+    SW_CUDA(ctx, cudaGetLastError());
+    int flagged = 0;
+    SW_CUDA(ctx, cudaMemcpy(&flagged, d_ovf_count, sizeof(int), cudaMemcpyDeviceToHost));
+    if ((size_t)flagged > s->ovf_cap)
+        SW_SET(ctx, SW_ERR_UNSUPPORTED, "%d overflow entries exceed the list (%zu)", flagged,
+               s->ovf_cap);
+    *rescored = (uint64_t)flagged;
+    return SW_OK;
+}
+
+void scheduler(sw_ctx* ctx) {
+    sw_serve_state* s = ctx->serve;
+    cudaSetDevice(ctx->device);
+    std::vector<int> finishing;
+    while (true) {
+        {
+            std::unique_lock<std::mutex> lock(s->mu);
+            bool any = false;
+            for (const Slot& x : s->slots) any |= x.used;
+            if (!any)
+                s->cv_work.wait(lock, [&] { return s->stopping || !s->pending.empty(); });
+            // admission: free slots take waiting requests, oldest first
+            const double t_adm = now_ms();
+            for (int i = 0; i < s->n_slots && !s->pending.empty(); ++i) {
+                Slot& x = s->slots[i];
+                if (x.used) continue;
+                x.used = true;
+                x.fresh = true;
+                x.done_chunks = 0;
+                x.req = std::move(s->pending.front());
+                s->pending.pop_front();
+                x.req.start_ms = t_adm;
+                ++s->stats.admitted;
+            }
+            any = false;
+            for (const Slot& x : s->slots) any |= x.used;
+            if (!any) {
+                if (s->stopping) break;
+                continue;
+            }
+        }
+        const double t0 = now_ms();
+        uint32_t launches = 0;
+        uint64_t rescored = 0;
+        const sw_status st = run_round(ctx, s, s->cursor, finishing, &launches, &rescored);
+        const double t1 = now_ms();
+        {
+            std::lock_guard<std::mutex> lock(s->mu);
+            ++s->stats.rounds;
+            s->stats.launches += launches;
+            s->stats.rescored += rescored;
+            s->stats.busy_ms += t1 - t0;
+            const int k = ctx->params.top_k;
+            if (st == SW_OK)
+                for (size_t f = 0; f < finishing.size(); ++f) {
+                    Slot& x = s->slots[(size_t)finishing[f]];
+                    for (int j = 0; j < k; ++j) {
+                        const unsigned long long key = s->h_keys[f * (size_t)k + j];
+                        if (key == 0ull) break;
+                        sw_hit h;
+                        h.score = (int32_t)(key >> 32);
+                        h.reserved = 0;
+                        h.index = 0xffffffffull - (key & 0xffffffffull);
+                        x.req.hits.push_back(h);
+                    }
+                }
+            for (Slot& x : s->slots) {
+                if (!x.used) continue;
+                x.fresh = false;
+                if (st == SW_OK && ++x.done_chunks < s->n_chunks) continue;
+                // cycle complete (its hits were read above), or the round failed
+                x.req.done_ms = t1;
+                x.req.status = st;
+                if (st == SW_OK) {
+                    s->stats.cells += (uint64_t)x.req.query.size() * ctx->n_residues;
+                    ++s->stats.completed;
+                } else {
+                    x.req.hits.clear();
+                    ++s->stats.failed;
+                }
+                s->done.push_back(std::move(x.req));
+                x.req = Request();
+                x.used = false;
+            }
+            s->cursor = (s->cursor + 1) % s->n_chunks;
+        }
+        s->cv_done.notify_all();
+    }
+}
+
+}  // namespace
+
+namespace swb {
+
+void serve_teardown(sw_ctx* ctx) {
+    sw_serve_state* s = ctx->serve;
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->stopping = true;
+        // waiting requests are dropped; requests in flight finish their cycle
+        s->pending.clear();
+    }
+    s->cv_work.notify_all();
+    if (s->th.joinable()) s->th.join();
+    serve_free(s);
+    delete s;
+    ctx->serve = nullptr;
+}
+
+}  // namespace swb
+
+extern "C" void sw_serve_options_default(sw_serve_options* o) {
+    if (!o) return;
+    o->max_active = 64;
+    o->chunks = 8;
+    o->max_pending = 0;
+    o->memory_budget = 0;
+    o->group_width = 16;
+    o->rows_per_thread = 64;
+    o->stack_rows = 4096;
+}
+
+extern "C" sw_status sw_serve_start(sw_ctx* ctx, const sw_serve_options* opt) {
+    if (!ctx) return SW_ERR_INVALID;
+    if (ctx->serve) SW_SET(ctx, SW_ERR_STATE, "already serving");
+    if (!ctx->db_loaded) SW_SET(ctx, SW_ERR_STATE, "no DB loaded (call sw_db_load first)");
+    SW_CUDA(ctx, cudaSetDevice(ctx->device));
+    sw_serve_options o;
+    sw_serve_options_default(&o);
+    if (opt) o = *opt;
+    const WfKernel* k = find_kernel(o.group_width, o.rows_per_thread);
+    if (!k || o.max_active == 0 || o.chunks == 0 || o.stack_rows < 0)
+        SW_SET(ctx, SW_ERR_INVALID, "bad serving options");
+    const int rows_big = (int)std::max<uint32_t>(kServeMaxQuery, (uint32_t)o.stack_rows);
+    if (shape_occupancy(ctx, *k, rows_big) == 0)
+        SW_SET(ctx, SW_ERR_UNSUPPORTED, "shape %dx%d cannot hold a stack of %d rows",
+               o.group_width, o.rows_per_thread, rows_big);
+    const int n_rec = (int)ctx->n_records;
+    if ((uint64_t)o.max_active * (uint64_t)std::max(n_rec, 1) >= (1ull << 31))
+        SW_SET(ctx, SW_ERR_UNSUPPORTED, "max_active x records reaches 2^31");
+    // slots: at most max_active, and as many as the memory budget holds at one
+    // score row plus its share of the key buffers each
+    const long long nblk0 = std::max<long long>(1, ((long long)n_rec + kTopkKeys - 1) / kTopkKeys);
+    const size_t per_slot = (size_t)std::max(n_rec, 1) * 4 + 2 * (size_t)nblk0 * kMaxTopK * 8 +
+                            (size_t)ctx->params.top_k * 8;
+    size_t free_b = 0, total_b = 0;
+    SW_CUDA(ctx, cudaMemGetInfo(&free_b, &total_b));
+    const size_t budget = o.memory_budget ? (size_t)o.memory_budget : free_b / 2;
+    if (budget / per_slot == 0)
+        SW_SET(ctx, SW_ERR_NOMEM, "the memory budget (%zu bytes) holds no request (%zu bytes each)",
+               budget, per_slot);
+    sw_serve_state* s = new sw_serve_state();
+    s->opt = o;
+    s->k = k;
+    s->n_slots = (int)std::min<size_t>(o.max_active, budget / per_slot);
+    s->occ_max = shape_occupancy(ctx, *k, k->R);
+    const int64_t npairs = ctx->n_pairs;
+    s->n_chunks = (int)std::max<int64_t>(1, std::min<int64_t>(o.chunks, std::max<int64_t>(npairs, 1)));
+    auto fail = [&](const char* what) {
+        serve_free(s);
+        delete s;
+        ctx->err = std::string("device allocation failed: serving ") + what;
+        return SW_ERR_NOMEM;
+    };
+    // the ring: pairs dealt round-robin (every n_chunks-th pair of the
+    // length-sorted order) and stored chunk after chunk
+    std::vector<Pair2> host_pairs((size_t)npairs);
+    if (npairs && cudaMemcpy(host_pairs.data(), ctx->d_pairs, (size_t)npairs * sizeof(Pair2),
+                             cudaMemcpyDeviceToHost) != cudaSuccess)
+        return fail("pair ring");
+    std::vector<Pair2> ring;
+    std::vector<uint32_t> ids;
+    ring.reserve((size_t)npairs);
+    ids.reserve((size_t)npairs);
+    s->chunk_begin.assign(1, 0);
+    for (int c = 0; c < s->n_chunks; ++c) {
+        for (int64_t p = c; p < npairs; p += s->n_chunks) {
+            ring.push_back(host_pairs[(size_t)p]);
+            ids.push_back((uint32_t)p);
+        }
+        s->chunk_begin.push_back((int)ring.size());
+    }
+    if (dev_alloc(&s->d_pairs, ring.size()) != cudaSuccess ||
+        dev_alloc(&s->d_pair_ids, ids.size()) != cudaSuccess)
+        return fail("pair ring");
+    if (!ring.empty() &&
+        (cudaMemcpy(s->d_pairs, ring.data(), ring.size() * sizeof(Pair2), cudaMemcpyHostToDevice) !=
+             cudaSuccess ||
+         cudaMemcpy(s->d_pair_ids, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess))
+        return fail("pair ring");
+    if (dev_alloc(&s->d_scores, (size_t)s->n_slots * std::max(n_rec, 1)) != cudaSuccess ||
+        dev_alloc(&s->d_counters, (size_t)s->n_slots + 1) != cudaSuccess)
+        return fail("slots");
+    // overflow entries: one per (request, record) at worst, bounded
+    s->ovf_cap = std::min<size_t>((size_t)s->n_slots * std::max(n_rec, 1),
+                                  std::max<size_t>((size_t)4 * std::max(n_rec, 1), (size_t)1 << 22));
+    if (dev_alloc(&s->d_ovf, s->ovf_cap) != cudaSuccess) return fail("overflow list");
+    if (dev_alloc(&s->d_keys[0], (size_t)s->n_slots * nblk0 * kMaxTopK) != cudaSuccess ||
+        dev_alloc(&s->d_keys[1], (size_t)s->n_slots * nblk0 * kMaxTopK) != cudaSuccess)
+        return fail("key buffers");
+    s->bnd_group = 2 * (size_t)std::max(ctx->max_cols, 8);
+    const size_t groups = (size_t)std::max(s->occ_max, 1) * ctx->num_sms * (k->block / k->T);
+    if (dev_alloc(&s->d_bnd, groups * s->bnd_group) != cudaSuccess) return fail("boundary rows");
+    if (cudaMallocHost((void**)&s->h_keys,
+                       (size_t)s->n_slots * ctx->params.top_k * sizeof(unsigned long long)) !=
+        cudaSuccess)
+        return fail("pinned keys");
+    s->slots.assign((size_t)s->n_slots, Slot());
+    s->stats.slots = (uint32_t)s->n_slots;
+    s->stats.chunks = (uint32_t)s->n_chunks;
+    ctx->serve = s;
+    s->th = std::thread(scheduler, ctx);
+    return SW_OK;
+}
+
+extern "C" sw_status sw_serve_submit(sw_ctx* ctx, uint64_t request_id, const uint8_t* query,
+                                     uint32_t qlen) {
+    if (!ctx || (qlen && !query)) return SW_ERR_INVALID;
+    sw_serve_state* s = ctx->serve;
+    if (!s) return SW_ERR_STATE;
+    if (qlen == 0 || qlen > kServeMaxQuery) return SW_ERR_UNSUPPORTED;
+    for (uint32_t i = 0; i < qlen; ++i)
+        if (query[i] > 24) return SW_ERR_INVALID;
+    Request r;
+    r.id = request_id;
+    r.query.assign(query, query + qlen);
+    r.submit_ms = now_ms();
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        if (s->stopping) return SW_ERR_STATE;
+        if (s->opt.max_pending && s->pending.size() >= s->opt.max_pending) return SW_ERR_BUSY;
+        s->pending.push_back(std::move(r));
+        ++s->stats.submitted;
+    }
+    s->cv_work.notify_one();
+    return SW_OK;
+}
+
+extern "C" sw_status sw_serve_poll(sw_ctx* ctx, uint32_t max_results, sw_serve_result* results,
+                                   sw_hit* hits, uint32_t* n_results, int32_t timeout_ms) {
+    if (!ctx || !n_results || (max_results && (!results || !hits))) return SW_ERR_INVALID;
+    *n_results = 0;
+    sw_serve_state* s = ctx->serve;
+    if (!s) return SW_ERR_STATE;
+    std::unique_lock<std::mutex> lock(s->mu);
+    if (s->done.empty() && timeout_ms != 0) {
+        auto ready = [&] { return !s->done.empty(); };
+        if (timeout_ms < 0)
+            s->cv_done.wait(lock, ready);
+        else
+            s->cv_done.wait_for(lock, std::chrono::milliseconds(timeout_ms), ready);
+    }
+    const int k = ctx->params.top_k;
+    uint32_t n = 0;
+    while (n < max_results && !s->done.empty()) {
+        Request& r = s->done.front();
+        results[n].request_id = r.id;
+        results[n].status = (int32_t)r.status;
+        results[n].n_hits = (uint32_t)r.hits.size();
+        results[n].submit_ms = r.submit_ms;
+        results[n].start_ms = r.start_ms;
+        results[n].done_ms = r.done_ms;
+        for (int j = 0; j < k; ++j)
+            hits[(size_t)n * k + j] = j < (int)r.hits.size() ? r.hits[(size_t)j] : sw_hit{0, 0, 0};
+        s->done.pop_front();
+        ++n;
+    }
+    *n_results = n;
+    return SW_OK;
+}
+
+extern "C" sw_status sw_serve_get_stats(sw_ctx* ctx, sw_serve_stats* out) {
+    if (!ctx || !out) return SW_ERR_INVALID;
+    sw_serve_state* s = ctx->serve;
+    if (!s) return SW_ERR_STATE;
+    std::lock_guard<std::mutex> lock(s->mu);
+    *out = s->stats;
+    out->pending = (uint32_t)s->pending.size();
+    uint32_t active = 0;
+    for (const Slot& x : s->slots) active += x.used ? 1u : 0u;
+    out->active = active;
+    return SW_OK;
+}
+
+extern "C" double sw_serve_clock_ms(void) { return now_ms(); }
+
+extern "C" sw_status sw_serve_stop(sw_ctx* ctx) {
+    if (!ctx) return SW_ERR_INVALID;
+    if (!ctx->serve) return SW_ERR_STATE;
+    serve_teardown(ctx);
+    return SW_OK;
+}

@@ -494,8 +494,8 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_batch(const BatchArgs a) {
         RunArgs r;
         r.db = a.db;
         r.pairs = a.pairs;
-        r.pair_begin = a.stack_pairs ? a.stack_pairs[2 * i] : a.pair_begin;
-        r.pair_count = a.stack_pairs ? a.stack_pairs[2 * i + 1] : a.pair_count;
+        r.pair_begin = a.pair_begin;
+        r.pair_count = a.pair_count;
         r.counter = a.counters + i;
         r.P = P;
         r.bias2 = a.bias2;
