@@ -69,6 +69,8 @@ def parse():
                     help="skip the batched (64-query) measurement")
     ap.add_argument("--serve-requests", type=int, default=96,
                     help="requests per offered load in the serving leg (0 = skip it)")
+    ap.add_argument("--no-stress", action="store_true",
+                    help="skip the overflow / long-record stress measurement")
     ap.add_argument("--kernel-only", action="store_true",
                     help="time the resident path only (no e2e, probe or CPU baseline)")
     return ap.parse_args()
@@ -337,6 +339,52 @@ def serve_leg(ctx, db, n_req: int, seed: int = 5):
     }
 
 
+def stress_leg(local_rank: int, steps: int):
+    """Overflow / long-record stress: 100,000 records + 1 % long (10,000..40,000)
+    with 0.5 % planted homologs of eight queries of 500..4,000 residues; GCUPS
+    of the resident path, and how many records the reference's int8 pass
+    would hand to its int16 re-score (score >= 117) on the same inputs."""
+    import torch
+    from swhybrid_b200 import capi, synth as _synth
+    db, queries, picks, _ = _synth.stress_workload()
+    ctx = capi.Context(local_rank, capi.default_params(top_k=10))
+    try:
+        ctx.load_db(db.residues, db.offsets)
+        from swhybrid_b200 import autotune
+        autotune.apply(ctx)
+        over8 = 0
+        for q in queries:
+            _, sc = ctx.search(q, want_scores=True)
+            over8 += int((sc >= 117).sum())
+        stream = torch.cuda.Stream(device=local_rank)
+        ctx.set_stream(stream.cuda_stream)
+        dq = [torch.from_numpy(q.copy()).to(f"cuda:{local_rank}") for q in queries]
+        for q in dq:
+            ctx.search_device(q.data_ptr(), q.numel())
+        ctx.sync()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for _ in range(steps):
+            for q in dq:
+                ctx.search_device(q.data_ptr(), q.numel())
+        ev1.record(stream)
+        ctx.sync()
+        torch.cuda.synchronize()
+        ms = ev0.elapsed_time(ev1)
+        cells = sum(len(q) for q in queries) * int(db.offsets[-1]) * steps
+        return {
+            "workload": "100,000 records lognormal(5.6,0.6) 20..5,000 + 1% uniform 10,000..40,000, "
+                        "0.5% homologs of the queries (sub 10..30%, indels 2%), 8 queries 500..4,000",
+            "n_residues": int(db.offsets[-1]), "planted": int(len(picks)),
+            "value": round(cells / (ms * 1e-3) / 1e9, 1), "unit": "GCUPS",
+            "ms_per_pass_of_8": round(ms / steps, 2),
+            "records_over_int8_range": over8,
+        }
+    finally:
+        ctx.close()
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     from swhybrid_b200 import capi
@@ -481,6 +529,11 @@ def run_ours(args, rank, world, local_rank):
         ctx.set_stream(None)
         served = serve_leg(ctx, db, args.serve_requests)
 
+    # ---- overflow / long-record stress (its own DB and context) ----
+    stress = None
+    if args.workload == "full" and not args.no_stress:
+        stress = stress_leg(local_rank, args.steps)
+
     # ---- correctness spot check on the resident DB (rank 0, cheap) ----
     spot = None
     if rank == 0 and args.workload == "small":
@@ -548,6 +601,8 @@ def run_ours(args, rank, world, local_rank):
             line["batched"] = batched
         if served is not None:
             line["served"] = served
+        if stress is not None:
+            line["stress"] = stress
     ctx.close()
     return line, db, queries
 

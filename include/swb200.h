@@ -251,8 +251,9 @@ typedef struct sw_serve_options {
     int32_t stack_rows;       /* requests shorter than this share stacks */
 } sw_serve_options;
 
-/* Defaults: 64 slots, 8 chunks, unbounded queue, half the free memory,
- * shape 16x64, stacks of 4096 rows. */
+/* Defaults: 128 slots, 4 chunks, unbounded queue, half the free memory,
+ * shape 16x64, stacks of 4096 rows (the best saturated throughput measured
+ * on B200 for requests of 30..8,000 residues against a 205 M-residue DB). */
 void sw_serve_options_default(sw_serve_options *opt);
 
 typedef struct sw_serve_result {

@@ -452,8 +452,8 @@ void serve_teardown(sw_ctx* ctx) {
 
 extern "C" void sw_serve_options_default(sw_serve_options* o) {
     if (!o) return;
-    o->max_active = 64;
-    o->chunks = 8;
+    o->max_active = 128;
+    o->chunks = 4;
     o->max_pending = 0;
     o->memory_budget = 0;
     o->group_width = 16;

@@ -188,3 +188,29 @@ def batched_queries(seed: int = 3, n: int = 64, lo: int = 50, hi: int = 5000):
 
 def poisson_arrivals(rng, n: int, rate_per_s: float) -> np.ndarray:
     return np.cumsum(rng.exponential(1.0 / rate_per_s, size=n))
+
+
+STRESS_QLENS = (500, 700, 1000, 1400, 1900, 2500, 3200, 4000)
+
+
+def stress_workload(seed: int = 4, n: int = 100_000, homolog_rate: float = 0.005):
+    """Overflow / long-record stress: ``stress_db`` records, eight queries of
+    500..4,000 residues, and ``homolog_rate`` of the records replaced by
+    homologs of the queries (an equal share each; substitutions uniform on
+    10..30 %, indels 2 %).  Returns (db, queries, planted record ids, owner
+    query of each planted id)."""
+    rng = np.random.default_rng(seed)
+    queries = [residues(rng, L) for L in STRESS_QLENS]
+    db, _ = stress_db(seed, n)
+    per_q = max(1, int(round(homolog_rate * db.n / len(queries))))
+    picks = rng.choice(db.n, size=per_q * len(queries), replace=False)
+    recs = [db.record(i) for i in range(db.n)]
+    owner = {}
+    for j, i in enumerate(picks):
+        q = j // per_q
+        recs[i] = mutate(rng, queries[q], rng.uniform(0.10, 0.30), 0.02)
+        owner[int(i)] = q
+    lens = np.array([len(r) for r in recs], dtype=np.int64)
+    off = np.zeros(db.n + 1, dtype=np.uint64)
+    off[1:] = np.cumsum(lens)
+    return DB(np.concatenate(recs).astype(np.uint8), off), queries, np.sort(picks), owner
