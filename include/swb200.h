@@ -66,8 +66,13 @@ typedef struct sw_hit {
  * (4..32 threads, a warp-cooperative anti-diagonal wavefront; narrow groups
  * behave like the reference's one-record-per-thread "inter-sequence" form,
  * wide groups are the "intra-sequence" form); rows_per_thread query rows are
- * kept in registers per thread (an even number).  Pairs of records with more than cutover
- * columns use the long shape, the rest the short shape. */
+ * kept in registers per thread (an even number).  Pairs of records with more
+ * than cutover columns run concurrently in the long-pair kernel, whose query
+ * passes are pipelined across the warps of a block: the long shape's rows per
+ * thread when it is 32 x {8, 16, 24, 32, 64}, otherwise chosen automatically.
+ * The rest use the short shape.  cutover 0: automatic (a split only when the
+ * DB's longest pairs would dominate the bulk launch, else one shape -- the
+ * long one -- for the whole DB).  sw_run_stats.used reports what ran. */
 typedef struct sw_kernel_config {
     int32_t long_group_width;
     int32_t long_rows_per_thread;
@@ -93,6 +98,8 @@ typedef struct sw_run_stats {
     uint32_t launches;      /* kernels this library launched in the last call */
     uint32_t queries;
     sw_kernel_config used;  /* shape of the last plain search */
+    double long_ms;         /* last plain search with a cut-over: long-pair launch time */
+    double bulk_ms;         /* ... and the concurrent bulk launch time (else 0, 0) */
 } sw_run_stats;
 
 /* ---- parameters, encoding ------------------------------------------------ */

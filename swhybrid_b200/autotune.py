@@ -45,7 +45,7 @@ def time_shape(ctx: capi.Context, dq, qlen: int, cfg: tuple, reps: int = 2) -> f
 
 
 def sweep(ctx: capi.Context, lengths, shapes=None, reps: int = 2, log=print,
-          cutovers=(2048, 4096, 8192, 16384)):
+          cutovers=(1024, 2048, 4096, 8192, 16384)):
     import torch
     shapes = shapes or [(T, R) for T in GROUP_WIDTHS for R in ROWS]
     results = {}

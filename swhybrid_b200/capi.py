@@ -112,7 +112,8 @@ class sw_run_stats(ctypes.Structure):
                 ("total_ms", ctypes.c_double),
                 ("cells", ctypes.c_uint64), ("rescored", ctypes.c_uint64),
                 ("launches", ctypes.c_uint32), ("queries", ctypes.c_uint32),
-                ("used", sw_kernel_config)]
+                ("used", sw_kernel_config), ("long_ms", ctypes.c_double),
+                ("bulk_ms", ctypes.c_double)]
 
 
 _lib = None

@@ -27,6 +27,7 @@
 #include "sw_aux.h"
 #include "sw_device.cuh"
 #include "sw_engine.h"
+#include "sw_long.h"
 #include "sw_registry.h"
 
 namespace swb {
@@ -180,6 +181,7 @@ extern "C" sw_status sw_ctx_create(int device, const sw_params* params, sw_ctx**
     if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return fail(SW_ERR_CUDA);
     ctx->num_sms = prop.multiProcessorCount;
     ctx->max_smem = (int)prop.sharedMemPerBlockOptin;
+    ctx->regs_per_sm = prop.regsPerMultiprocessor;
     if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess)
         return fail(SW_ERR_CUDA);
     ctx->stream = ctx->own_stream;
@@ -212,6 +214,15 @@ extern "C" sw_status sw_ctx_create(int device, const sw_params* params, sw_ctx**
             cudaFuncSetAttribute(ks[i].batch_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  ctx->max_smem) != cudaSuccess)
             return fail(SW_ERR_CUDA);
+    // the long-pair kernels also hold a few static shared words
+    const LongKernel* lks = long_kernels(&nk);
+    for (int i = 0; i < nk; ++i) {
+        cudaFuncAttributes fa;
+        if (cudaFuncGetAttributes(&fa, lks[i].fn) != cudaSuccess ||
+            cudaFuncSetAttribute(lks[i].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 ctx->max_smem - (int)fa.sharedSizeBytes) != cudaSuccess)
+            return fail(SW_ERR_CUDA);
+    }
     *out = ctx;
     return SW_OK;
 }
@@ -330,7 +341,11 @@ extern "C" sw_status sw_db_load(sw_ctx* ctx, const uint8_t* residues, const uint
     ctx->max_len = maxlen;
     ctx->units = units;
     ctx->pair_ncols.resize(nonempty);
-    for (uint64_t p = 0; p < nonempty; ++p) ctx->pair_ncols[p] = pairs[p].ncols;
+    ctx->pair_cols_total = 0;
+    for (uint64_t p = 0; p < nonempty; ++p) {
+        ctx->pair_ncols[p] = pairs[p].ncols;
+        ctx->pair_cols_total += pairs[p].ncols;
+    }
     auto nomem = [&](const char* what) {
         free_db(ctx);
         ctx->err = std::string("device allocation failed: ") + what;
@@ -507,6 +522,68 @@ sw_status take_marks(sw_ctx* ctx, sw_ctx::Marks* m) {
     return SW_OK;
 }
 
+// Cut-over for a configuration without one: a DB whose longest pair needs more
+// than twice the column steps an evenly loaded bulk group gets (the bulk
+// launch would end on a few serial chains) sends the pairs above a quarter of
+// that share to the long-pair kernel; otherwise no split.
+int auto_cutover(sw_ctx* ctx, const sw_kernel_config& cfg, int qlen) {
+    if (ctx->n_pairs == 0) return 0;
+    const WfKernel* k = find_kernel(cfg.short_group_width, cfg.short_rows_per_thread);
+    if (!k) return 0;
+    const int occ = std::max(1, shape_occupancy(ctx, *k, qlen));
+    const double groups = (double)occ * ctx->num_sms * (k->block / k->T);
+    const double share = (double)ctx->pair_cols_total / groups;
+    if ((double)ctx->pair_ncols[0] <= 2.0 * share) return 0;
+    return std::max(1024, (int)(share / 4));
+}
+
+// The long-pair kernel for a query: the configured long shape when it is a
+// compiled sw_long row count (group width 32) whose passes fit one pipeline,
+// else the smallest row count that needs at most 3 passes (measured on B200:
+// 2-3 passes per pair balance pipeline parallelism against per-step
+// overhead), else at most kLongMaxPasses.  A block takes a whole SM:
+// *pipelines is how many pipelines of *passes warps fit its registers and
+// shared memory.  Returns null when nothing fits.
+const LongKernel* choose_long(sw_ctx* ctx, const sw_kernel_config& cfg, int qlen, int* passes,
+                              int* pipelines, size_t* smem_bytes) {
+    int n = 0;
+    const LongKernel* lk = long_kernels(&n);
+    auto fits = [&](const LongKernel& k) {
+        const int P = (qlen + 32 * k.R - 1) / (32 * k.R);
+        if (P > kLongMaxPasses) return false;
+        cudaFuncAttributes fa;
+        if (cudaFuncGetAttributes(&fa, k.fn) != cudaSuccess) {
+            cudaGetLastError();
+            return false;
+        }
+        const size_t dyn = (size_t)ctx->max_smem - fa.sharedSizeBytes;
+        const int warp_regs = (fa.numRegs + 7) / 8 * 8 * 32;
+        int G = std::min(k.max_threads / 32, ctx->regs_per_sm / std::max(warp_regs, 1)) / P;
+        while (G > 0 && k.smem(P, G) > dyn) --G;
+        while (G > 0) {
+            int nb = 0;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k.fn, G * P * 32, dyn) ==
+                    cudaSuccess && nb >= 1)
+                break;
+            cudaGetLastError();
+            --G;
+        }
+        if (G == 0) return false;
+        *passes = P;
+        *pipelines = G;
+        *smem_bytes = dyn;
+        return true;
+    };
+    if (cfg.long_group_width == 32)
+        for (int i = 0; i < n; ++i)
+            if (lk[i].R == cfg.long_rows_per_thread && fits(lk[i])) return &lk[i];
+    for (int i = 0; i < n; ++i)
+        if ((qlen + 32 * lk[i].R - 1) / (32 * lk[i].R) <= 3 && fits(lk[i])) return &lk[i];
+    for (int i = 0; i < n; ++i)
+        if (fits(lk[i])) return &lk[i];
+    return nullptr;
+}
+
 sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t* d_scores_rec,
                          unsigned long long** keys_final, uint32_t* launches) {
     cudaStream_t st = ctx->stream;
@@ -524,9 +601,11 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
     SW_CUDA(ctx, cudaEventRecord(mk.e[1], st));
     // pairs [0, n_long) are longer than the cut-over
     int64_t n_long = ctx->n_pairs;
-    if (cfg.cutover > 0) {
+    const int cutover = cfg.cutover > 0 ? cfg.cutover : auto_cutover(ctx, cfg, qlen);
+    ctx->stats.used.cutover = cutover;
+    if (cutover > 0) {
         n_long = 0;
-        while (n_long < ctx->n_pairs && (int)ctx->pair_ncols[n_long] > cfg.cutover) ++n_long;
+        while (n_long < ctx->n_pairs && (int)ctx->pair_ncols[n_long] > cutover) ++n_long;
     }
     struct Seg {
         int T, R;
@@ -536,27 +615,76 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
                  {cfg.short_group_width, cfg.short_rows_per_thread, n_long, ctx->n_pairs, 1}};
     const int ovf_thresh = 32767 - std::max(ctx->max_score, 1) + 1;
     // With a cut-over, the long pairs run concurrently on the side stream in
-    // blocks of 128 threads that request the whole shared memory of an SM:
-    // each such SM then holds one of them and nothing else, so the few long
-    // pairs (whose steps are inherently serial) get a warp scheduler each
-    // instead of queueing behind the bulk; the bulk takes the other SMs.
-    const bool split = cfg.cutover > 0 && n_long > 0 && n_long < ctx->n_pairs;
+    // sw_long blocks (one warp per query pass, the passes of a pair pipelined
+    // across warps, several pipelines per block, one block per SM) on SMs the
+    // bulk grid leaves free, as many SMs as the long pairs' share of the
+    // columns.
+    bool split = cutover > 0 && n_long > 0 && n_long < ctx->n_pairs;
+    const LongKernel* lk = nullptr;
+    int lpasses = 0, lpipes = 0;
+    size_t lsmem = 0;
     if (split) {
-        SW_CUDA(ctx, cudaEventRecord(ctx->fork_ev, st));
-        SW_CUDA(ctx, cudaStreamWaitEvent(ctx->side_stream, ctx->fork_ev, 0));
-    }
-    // SMs the long launch reserves; the bulk grid leaves them free so the
-    // long blocks are placed whichever launch the hardware dispatches first
-    int reserved_sms = 0;
-    if (split) {
-        const WfKernel* kl = find_kernel(segs[0].T, segs[0].R);
-        if (kl) {
-            const int64_t gpb = std::max(128, kl->T) / kl->T;
-            reserved_sms = (int)std::max<int64_t>(
-                1, std::min<int64_t>((n_long + gpb - 1) / gpb, ctx->num_sms / 2));
+        lk = choose_long(ctx, cfg, qlen, &lpasses, &lpipes, &lsmem);
+        if (!lk) {          // no pipelined shape for this length: one launch for all
+            split = false;
+            segs[0].e = 0;
+            segs[1].b = 0;
+        } else {
+            ctx->stats.used.long_group_width = 32;
+            ctx->stats.used.long_rows_per_thread = lk->R;
         }
     }
-    for (int si = 0; si < 2; ++si) {
+    int reserved_sms = 0;
+    if (split) {
+        uint64_t long_cols = 0;
+        for (int64_t p = 0; p < n_long; ++p) long_cols += ctx->pair_ncols[p];
+        const double share = (double)long_cols / (double)std::max<uint64_t>(ctx->pair_cols_total, 1);
+        // SMs for the long launch: their share of the columns, or, when there
+        // are few long pairs, enough SMs that each warp scheduler runs about
+        // one of their warps (a pair's column steps are serial, so a crowded
+        // SM would make the longest pair the critical path), at most half
+        reserved_sms = (int)std::lround(share * ctx->num_sms);
+        const int64_t spread = (n_long * lpasses + 3) / 4;
+        reserved_sms = (int)std::max<int64_t>(reserved_sms,
+                                              std::min<int64_t>(spread, ctx->num_sms / 2));
+        reserved_sms = std::max(1, std::min(reserved_sms, ctx->num_sms - 1));
+        reserved_sms = (int)std::min<int64_t>(reserved_sms, (n_long + lpipes - 1) / lpipes);
+        // pipelines per block: the long pairs spread evenly over those SMs
+        lpipes = (int)std::min<int64_t>(lpipes, (n_long + reserved_sms - 1) / reserved_sms);
+        SW_CUDA(ctx, cudaEventRecord(ctx->fork_ev, st));
+        SW_CUDA(ctx, cudaStreamWaitEvent(ctx->side_stream, ctx->fork_ev, 0));
+        LongArgs la;
+        la.db = ctx->d_db;
+        la.pairs = ctx->d_pairs;
+        la.pair_begin = 0;
+        la.pair_count = (int)n_long;
+        la.counter = ctx->d_counters + segs[0].counter;
+        la.query = d_query;
+        la.qlen = qlen;
+        la.passes = lpasses;
+        la.mat = ctx->d_mat;
+        la.bias2 = (uint32_t)(ctx->params.gap_open + ctx->params.gap_extend);
+        la.bias2 |= la.bias2 << 16;
+        la.neg_e = (uint32_t)(uint16_t)(int16_t)(-ctx->params.gap_extend);
+        la.neg_e |= la.neg_e << 16;
+        la.one = 1u;
+        la.scores = ctx->d_scores;
+        la.n_records = (int)ctx->n_records;
+        la.ovf_list = ctx->d_ovf;
+        la.ovf_count = ctx->d_counters + 2;
+        la.ovf_thresh = ovf_thresh;
+        la.ovf_cap = (int)ctx->n_records + 1;
+        void* args[] = {&la};
+        SW_CUDA(ctx, cudaEventRecord(mk.e[4], ctx->side_stream));
+        SW_CUDA(ctx, cudaLaunchKernel(lk->fn, dim3((unsigned)reserved_sms),
+                                      dim3(lpasses * lpipes * 32), args, lsmem, ctx->side_stream));
+        SW_CUDA(ctx, cudaEventRecord(mk.e[5], ctx->side_stream));
+        ++*launches;
+        ++mk.fp_launches;
+        SW_CUDA(ctx, cudaEventRecord(mk.e[6], st));
+    }
+    mk.split = split;
+    for (int si = split ? 1 : 0; si < 2; ++si) {
         const Seg& sg = segs[si];
         if (sg.e <= sg.b) continue;
         const WfKernel* k = find_kernel(sg.T, sg.R);
@@ -586,27 +714,18 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
         a.ovf_list = ctx->d_ovf;
         a.ovf_count = ctx->d_counters + 2;
         a.ovf_thresh = ovf_thresh;
-        const int64_t groups_needed = (sg.e - sg.b);
         void* args[] = {&a};
-        if (split && si == 0) {
-            const int threads = std::max(128, k->T);
-            const int64_t gpb = threads / k->T;
-            int64_t grid = (groups_needed + gpb - 1) / gpb;
-            grid = std::max<int64_t>(1, std::min<int64_t>(grid, ctx->num_sms / 2));
-            SW_CUDA(ctx, cudaLaunchKernel(k->fn, dim3((unsigned)grid), dim3(threads), args,
-                                          (size_t)ctx->max_smem, ctx->side_stream));
-        } else {
-            int64_t grid = (int64_t)occ * (ctx->num_sms - reserved_sms);
-            const int64_t groups_per_block = k->block / k->T;
-            grid = std::min<int64_t>(grid, (groups_needed + groups_per_block - 1) / groups_per_block);
-            grid = std::max<int64_t>(grid, 1);
-            SW_CUDA(ctx, cudaLaunchKernel(k->fn, dim3((unsigned)grid), dim3(k->block), args,
-                                          k->smem(qlen), st));
-        }
+        int64_t grid = (int64_t)occ * (ctx->num_sms - reserved_sms);
+        const int64_t groups_per_block = k->block / k->T;
+        grid = std::min<int64_t>(grid, ((sg.e - sg.b) + groups_per_block - 1) / groups_per_block);
+        grid = std::max<int64_t>(grid, 1);
+        SW_CUDA(ctx, cudaLaunchKernel(k->fn, dim3((unsigned)grid), dim3(k->block), args,
+                                      k->smem(qlen), st));
         ++*launches;
         ++mk.fp_launches;
     }
     if (split) {
+        SW_CUDA(ctx, cudaEventRecord(mk.e[7], st));
         SW_CUDA(ctx, cudaEventRecord(ctx->join_ev, ctx->side_stream));
         SW_CUDA(ctx, cudaStreamWaitEvent(st, ctx->join_ev, 0));
     }
@@ -678,9 +797,15 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
 sw_status drain(sw_ctx* ctx, float* last_ms, float* last_fp_ms) {
     SW_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     for (auto& m : ctx->pending) {
-        float whole = 0.f, fp = 0.f;
+        float whole = 0.f, fp = 0.f, lms = 0.f, bms = 0.f;
         SW_CUDA(ctx, cudaEventElapsedTime(&whole, m.e[0], m.e[3]));
         SW_CUDA(ctx, cudaEventElapsedTime(&fp, m.e[1], m.e[2]));
+        if (m.split) {
+            SW_CUDA(ctx, cudaEventElapsedTime(&lms, m.e[4], m.e[5]));
+            SW_CUDA(ctx, cudaEventElapsedTime(&bms, m.e[6], m.e[7]));
+        }
+        ctx->stats.long_ms = lms;
+        ctx->stats.bulk_ms = bms;
         ctx->totals.search_ms += whole;
         ctx->totals.first_pass_ms += fp;
         ctx->totals.first_pass_launches += m.fp_launches;

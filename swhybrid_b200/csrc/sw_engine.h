@@ -46,14 +46,18 @@ struct sw_ctx {
     int device = 0;
     int num_sms = 0;
     int max_smem = 0;
+    int regs_per_sm = 0;
     cudaStream_t stream = nullptr;       // stream in use
     cudaStream_t own_stream = nullptr;   // the context's own stream
     cudaStream_t side_stream = nullptr;  // concurrent launch of the long-record pairs
     cudaEvent_t fork_ev = nullptr, join_ev = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     // timing events of enqueued searches: begin, first pass begin/end, end
+    // (and, with a cut-over, long launch begin/end on the side stream, bulk
+    // launch begin/end on the main stream)
     struct Marks {
-        cudaEvent_t e[4];
+        cudaEvent_t e[8];
+        bool split;
         uint32_t fp_launches;
         uint32_t launches;
         uint64_t cells;
@@ -75,6 +79,7 @@ struct sw_ctx {
     uint64_t units = 0;                // 16-byte units of the column stream
     uint64_t db_bytes = 0;
     std::vector<uint32_t> pair_ncols;  // host copy, for shape selection
+    uint64_t pair_cols_total = 0;      // sum of pair_ncols
     uint4* d_db = nullptr;
     swb::Pair2* d_pairs = nullptr;
     uint32_t* d_perm = nullptr;        // sorted position -> record

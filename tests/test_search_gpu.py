@@ -126,6 +126,65 @@ def test_long_records_and_many_passes(ctx):
     check_topk(hits, want)
 
 
+# compiled long-pair row counts, plus 48 (not compiled: the automatic choice)
+LONG_ROWS = (8, 16, 24, 32, 48, 64)
+
+
+@pytest.fixture(scope="module")
+def long_case():
+    """Records of 1,600..9,000 residues (long pairs) among short ones, with
+    planted homologs (scores far above the int8 range), and queries whose
+    pass count runs from 1 to the 8-warp maximum of the long-pair kernel."""
+    rng = np.random.default_rng(31)
+    lens = np.concatenate([rng.integers(1600, 9000, size=120), rng.integers(5, 600, size=900)])
+    lens = lens[rng.permutation(len(lens))]
+    db = synth.db_from_lengths(rng, lens)
+    queries = [synth.residues(rng, L) for L in (100, 700, 2100, 4097, 8000)]
+    db, _ = synth.plant_homologs(rng, db, queries[2], 0.02)
+    want = [oracle.search(q, db.residues, db.offsets, M, 12, 2) for q in queries]
+    return db, queries, want
+
+
+@pytest.mark.parametrize("rows", LONG_ROWS)
+def test_long_pair_pipeline_every_row_count(ctx, long_case, rows):
+    """Pairs above the cut-over go to the long-pair kernel (one warp per query
+    pass, passes pipelined through shared memory, several pipelines per
+    block); every row count and pass count must give the oracle's scores."""
+    db, queries, want = long_case
+    ctx.load_db(db.residues, db.offsets)
+    try:
+        ran = 0
+        for q, w in zip(queries, want):
+            if len(q) > 8 * 32 * rows:
+                continue
+            ctx.set_kernel_config((32, rows, 16, 16, 1500))
+            hits, scores = ctx.search(q, want_scores=True)
+            np.testing.assert_array_equal(scores, w, err_msg=f"R={rows} qlen={len(q)}")
+            check_topk(hits, w)
+            st = ctx.run_stats()
+            assert st.long_ms > 0 and st.bulk_ms > 0
+            assert st.used.cutover == 1500
+            ran += 1
+        assert ran >= 2
+    finally:
+        ctx.set_kernel_config(None)
+
+
+def test_automatic_cutover_on_a_long_tailed_db(ctx, long_case):
+    """Without a configured cut-over, a DB whose longest pairs dominate gets
+    one automatically, and the scores stay exact."""
+    db, queries, want = long_case
+    ctx.load_db(db.residues, db.offsets)
+    ctx.set_kernel_config((16, 16, 16, 16, 0))
+    try:
+        _, scores = ctx.search(queries[1], want_scores=True)
+        np.testing.assert_array_equal(scores, want[1])
+        st = ctx.run_stats()
+        assert st.used.cutover >= 1024 and st.long_ms > 0
+    finally:
+        ctx.set_kernel_config(None)
+
+
 def test_other_gap_costs_match_oracle():
     rng = np.random.default_rng(22)
     db = synth.small_db(5, 800)
