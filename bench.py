@@ -49,6 +49,8 @@ WORKLOADS = {
             "20 query lengths log-spaced 144..5,478, one query per call",
     "small": "plain method, small: 20,000 records (~6.5M residues), query 375",
     "profile": "profiling case: the full-size DB (~205M residues) and one query of 1,434",
+    "stress": "overflow/long-record stress: 100,000 records + 1% of 10,000..40,000 (~58M residues), "
+              "0.5% planted homologs, 8 queries 500..4,000, one query per call",
 }
 
 
@@ -84,6 +86,8 @@ def make_workload(name: str, rank: int):
     elif name == "profile":
         db = synth.full_db(2 + 1000 * rank)
         queries = [synth.query(112, 1434)]
+    elif name == "stress":
+        db, queries, _, _ = synth.stress_workload(4 + 1000 * rank)
     else:
         db = synth.full_db(2 + 1000 * rank)
         queries = [synth.query(100 + i, int(L)) for i, L in enumerate(synth.sweep_lengths())]
