@@ -236,6 +236,39 @@ sw_status sw_search_batch(struct sw_ctx *ctx, uint32_t n_queries, const uint8_t 
                           const uint64_t *query_offsets, sw_hit *hits, uint32_t *n_hits,
                           int32_t *scores);
 
+/* ---- alignments of chosen records ---------------------------------------- */
+
+/* One alignment: the best local alignment of the query against a record. */
+typedef struct sw_alignment {
+    uint64_t index;       /* the record (DB order, as given to sw_db_load) */
+    int32_t score;        /* its exact score (no 65535 cap) */
+    uint32_t q_begin;     /* aligned query residues [q_begin, q_end) */
+    uint32_t q_end;
+    uint32_t d_begin;     /* aligned record residues [d_begin, d_end) */
+    uint32_t d_end;
+    uint32_t matches;     /* aligned pairs with identical residues */
+    uint32_t n_ops;       /* CIGAR operations at ops[ops_offset ..] */
+    uint32_t reserved;
+    uint64_t ops_offset;
+} sw_alignment;
+
+/* No counterpart in the reference, which reports scores and titles only
+ * (WorkerPool::showResult, src/WorkerPool.cpp:130-155).  For each of the n
+ * records (typically the hits of a sw_search), the best local alignment of
+ * the query against it: coordinates and a CIGAR, computed on the device
+ * (exact int32 Gotoh with direction bits, then a walk back from the first
+ * maximal cell in record-then-query order; ties prefer the diagonal, then a
+ * gap in the query, then a gap in the record, and a gap opened over one
+ * extended).  ops receives run-length CIGAR operations in BAM's encoding,
+ * (length << 4) | op with op 0 = M, 1 = I (query residue against a gap),
+ * 2 = D (record residue against a gap); *ops_used receives how many were
+ * needed (SW_ERR_UNSUPPORTED when more than ops_cap).  Direction bits take
+ * qlen x record length / 2 bytes of device memory per record (at most 8 GiB
+ * per record; records are processed in rounds within that bound). */
+sw_status sw_traceback(struct sw_ctx *ctx, const uint8_t *query, uint32_t qlen,
+                       const uint64_t *records, uint32_t n, sw_alignment *out,
+                       uint32_t *ops, uint64_t ops_cap, uint64_t *ops_used);
+
 /* ---- serving ------------------------------------------------------------- */
 
 /* The reference serves no requests: src/main.cpp runs one query per process

@@ -56,6 +56,9 @@ def lib():
                                        _c_i32, _c_i32, _c_i32, _ptr]
         _lib.oracle_topk.restype = _c_i32
         _lib.oracle_topk.argtypes = [_ptr, _c_i64, _c_i32, _ptr, _ptr]
+        _lib.oracle_traceback.restype = _c_i64
+        _lib.oracle_traceback.argtypes = [_ptr, _c_i64, _ptr, _c_i64, _ptr, _c_i32, _c_i32,
+                                          _ptr, _ptr, _c_i64]
     return _lib
 
 
@@ -116,6 +119,38 @@ def search(query, residues, offsets, matrix, gap_oe=12, gap_e=2, mode=1,
     lib().oracle_search(_p(q), len(q), _p(r), _p(o), n, _p(m), gap_oe, gap_e,
                         mode, threads, _p(out))
     return out[:n]
+
+
+OPS = "MID"
+
+
+def traceback(q, d, matrix, gap_oe=12, gap_e=2):
+    """Best local alignment of q against d under the library's traceback
+    rules: dict(score, q_begin, q_end, d_begin, d_end, cigar)."""
+    q = np.ascontiguousarray(q, dtype=np.uint8)
+    d = np.ascontiguousarray(d, dtype=np.uint8)
+    m = _mat(matrix)
+    out = np.zeros(5, dtype=np.int64)
+    cap = len(q) + len(d) + 1
+    ops = np.zeros(cap, dtype=np.uint8)
+    n = lib().oracle_traceback(_p(q), len(q), _p(d), len(d), _p(m), gap_oe, gap_e, _p(out),
+                               _p(ops), cap)
+    assert n >= 0
+    return dict(score=int(out[0]), q_begin=int(out[1]), q_end=int(out[2]),
+                d_begin=int(out[3]), d_end=int(out[4]), cigar=cigar(ops[:n]))
+
+
+def cigar(ops) -> str:
+    """Run-length CIGAR text of a per-column op sequence (0 M, 1 I, 2 D)."""
+    out, prev, run = [], None, 0
+    for o in list(ops) + [None]:
+        if o == prev:
+            run += 1
+            continue
+        if prev is not None:
+            out.append(f"{run}{OPS[prev]}")
+        prev, run = o, 1
+    return "".join(out)
 
 
 def topk(scores, k):

@@ -149,3 +149,98 @@ int32_t oracle_topk(const int32_t *scores, int64_t n, int32_t k,
     }
     return m;
 }
+
+/* Traceback of the best local alignment (the reference reports scores only,
+ * so this restates the semantics the library's sw_traceback defines; the
+ * score it reaches is the Gotoh score above):
+ *   H(i,j) = max(0, H(i-1,j-1) + s(q_i, d_j), E(i,j), F(i,j))
+ *   E(i,j) = max(E(i,j-1) - e, H(i,j-1) - oe)   (d_j against a gap: 'D')
+ *   F(i,j) = max(F(i-1,j) - e, H(i-1,j) - oe)   (q_i against a gap: 'I')
+ *   H = 0 on row 0 and column 0, E and F below any reachable value there.
+ * End cell: the first cell with the maximal H in column-major order (DB
+ * position, then query position).  Walk back from it: in H, stop at H = 0,
+ * else prefer the diagonal, then E, then F; in E or F prefer "opened here"
+ * over "extended" when both give the value.  out = {score, q_begin, q_end,
+ * d_begin, d_end} (0-based, end exclusive); ops in alignment order, codes
+ * 0 = M (aligned pair), 1 = I (query residue, gap in DB), 2 = D (DB residue,
+ * gap in query).  Returns the number of ops, or -1 if ops_cap is too small. */
+int64_t oracle_traceback(const uint8_t *q, int64_t qlen, const uint8_t *d,
+                         int64_t dlen, const int32_t *mat, int32_t oe, int32_t e,
+                         int64_t *out, uint8_t *ops, int64_t ops_cap)
+{
+    const int64_t W = dlen + 1;
+    const int32_t NEG = -(1 << 28);
+    int32_t *H = (int32_t *)calloc((size_t)(qlen + 1) * W, sizeof(int32_t));
+    int32_t *E = (int32_t *)malloc((size_t)(qlen + 1) * W * sizeof(int32_t));
+    int32_t *F = (int32_t *)malloc((size_t)(qlen + 1) * W * sizeof(int32_t));
+    for (int64_t k = 0; k < (qlen + 1) * W; ++k) E[k] = F[k] = NEG;
+    int32_t best = 0;
+    int64_t bi = 0, bj = 0;
+    for (int64_t j = 1; j <= dlen; ++j)
+        for (int64_t i = 1; i <= qlen; ++i) {
+            const int32_t s = mat[(q[i - 1] & 31) * 32 + (d[j - 1] & 31)];
+            int32_t ev = E[i * W + j - 1] - e, eo = H[i * W + j - 1] - oe;
+            int32_t fv = F[(i - 1) * W + j] - e, fo = H[(i - 1) * W + j] - oe;
+            E[i * W + j] = ev > eo ? ev : eo;
+            F[i * W + j] = fv > fo ? fv : fo;
+            int32_t h = H[(i - 1) * W + j - 1] + s;
+            if (h < E[i * W + j]) h = E[i * W + j];
+            if (h < F[i * W + j]) h = F[i * W + j];
+            if (h < 0) h = 0;
+            H[i * W + j] = h;
+            if (h > best) {
+                best = h;
+                bi = i;
+                bj = j;
+            }
+        }
+    out[0] = best;
+    out[1] = out[2] = bi;
+    out[3] = out[4] = bj;
+    int64_t n = 0;
+    if (best > 0) {
+        int64_t i = bi, j = bj, si = bi, sj = bj;
+        int state = 0;   /* 0 H, 1 E, 2 F */
+        while (1) {
+            if (n >= ops_cap) { n = -1; break; }
+            if (state == 0) {
+                if (i == 0 || j == 0 || H[i * W + j] == 0) break;
+                const int32_t s = mat[(q[i - 1] & 31) * 32 + (d[j - 1] & 31)];
+                if (H[i * W + j] == H[(i - 1) * W + j - 1] + s) {
+                    ops[n++] = 0;
+                    si = i;
+                    sj = j;
+                    --i;
+                    --j;
+                } else if (H[i * W + j] == E[i * W + j]) {
+                    state = 1;
+                } else {
+                    state = 2;
+                }
+            } else if (state == 1) {
+                ops[n++] = 2;
+                const int open = H[i * W + j - 1] - oe >= E[i * W + j - 1] - e;
+                --j;
+                state = open ? 0 : 1;
+            } else {
+                ops[n++] = 1;
+                const int open = H[(i - 1) * W + j] - oe >= F[(i - 1) * W + j] - e;
+                --i;
+                state = open ? 0 : 2;
+            }
+        }
+        if (n > 0) {
+            for (int64_t a = 0, b = n - 1; a < b; ++a, --b) {
+                uint8_t t = ops[a];
+                ops[a] = ops[b];
+                ops[b] = t;
+            }
+        }
+        out[1] = si - 1;
+        out[3] = sj - 1;
+    }
+    free(H);
+    free(E);
+    free(F);
+    return n;
+}

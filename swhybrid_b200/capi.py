@@ -31,6 +31,7 @@ EXPORTS = [
     "sw_set_tuning", "sw_score_noalloc", "sw_get_shapes", "sw_set_batch_options",
     "sw_search_batch", "sw_serve_options_default", "sw_serve_start", "sw_serve_submit",
     "sw_serve_poll", "sw_serve_get_stats", "sw_serve_clock_ms", "sw_serve_stop",
+    "sw_traceback",
 ]
 
 
@@ -66,6 +67,14 @@ class sw_batch_options(ctypes.Structure):
                 ("long_rows_per_thread", ctypes.c_int32), ("use_graph", ctypes.c_int32),
                 ("group_width", ctypes.c_int32), ("rows_per_thread", ctypes.c_int32),
                 ("stack_rows", ctypes.c_int32)]
+
+
+class sw_alignment(ctypes.Structure):
+    _fields_ = [("index", ctypes.c_uint64), ("score", ctypes.c_int32),
+                ("q_begin", ctypes.c_uint32), ("q_end", ctypes.c_uint32),
+                ("d_begin", ctypes.c_uint32), ("d_end", ctypes.c_uint32),
+                ("matches", ctypes.c_uint32), ("n_ops", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("ops_offset", ctypes.c_uint64)]
 
 
 class sw_serve_options(ctypes.Structure):
@@ -177,6 +186,10 @@ def load(path: str = LIB_PATH):
     L.sw_score_noalloc.argtypes = [ctypes.c_int, ctypes.POINTER(sw_params), ctypes.c_void_p,
                                    ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                    ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]
+    L.sw_traceback.restype = ctypes.c_int
+    L.sw_traceback.argtypes = [P, P, ctypes.c_uint32, P, ctypes.c_uint32,
+                               ctypes.POINTER(sw_alignment), P, ctypes.c_uint64,
+                               ctypes.POINTER(ctypes.c_uint64)]
     L.sw_serve_options_default.restype = None
     L.sw_serve_options_default.argtypes = [ctypes.POINTER(sw_serve_options)]
     L.sw_serve_start.restype = ctypes.c_int
@@ -363,6 +376,36 @@ class Context:
         t = sw_totals()
         self._check(self.L.sw_get_totals(self.h, ctypes.byref(t)), "sw_get_totals")
         return t
+
+    def traceback(self, query: np.ndarray, records) -> list:
+        """Best local alignment of the query against each record (DB order
+        indices): dicts with index, score, q_begin, q_end, d_begin, d_end,
+        matches, cigar (text, M/I/D)."""
+        q = np.ascontiguousarray(query, dtype=np.uint8)
+        recs = np.ascontiguousarray(records, dtype=np.uint64)
+        n = len(recs)
+        out = (sw_alignment * max(n, 1))()
+        cap = 64 * max(n, 1)
+        while True:
+            ops = np.zeros(cap, dtype=np.uint32)
+            used = ctypes.c_uint64(0)
+            st = self.L.sw_traceback(self.h, _ptr(q) if q.size else None, q.size,
+                                     _ptr(recs) if n else None, n, out, _ptr(ops), cap,
+                                     ctypes.byref(used))
+            if st == 6 and used.value > cap:     # ops buffer too small: size it and repeat
+                cap = int(used.value)
+                continue
+            self._check(st, "sw_traceback")
+            break
+        res = []
+        for i in range(n):
+            a = out[i]
+            cig = "".join(f"{int(o) >> 4}{'MID'[int(o) & 15]}"
+                          for o in ops[a.ops_offset:a.ops_offset + a.n_ops])
+            res.append(dict(index=int(a.index), score=a.score, q_begin=a.q_begin,
+                            q_end=a.q_end, d_begin=a.d_begin, d_end=a.d_end,
+                            matches=a.matches, cigar=cig))
+        return res
 
     # ---- serving ----------------------------------------------------------
     def serve_start(self, max_active=None, chunks=None, max_pending=None, memory_budget=None,

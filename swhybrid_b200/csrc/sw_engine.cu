@@ -229,6 +229,9 @@ extern "C" sw_status sw_ctx_create(int device, const sw_params* params, sw_ctx**
 
 static void free_db(sw_ctx* ctx) {
     swb::free_batch(ctx);
+    swb::free_traceback(ctx);
+    ctx->rec_pos.clear();
+    ctx->rec_len.clear();
     dev_free(ctx->d_rs_scratch);
     dev_free(ctx->d_db);
     dev_free(ctx->d_pairs);
@@ -334,6 +337,9 @@ extern "C" sw_status sw_db_load(sw_ctx* ctx, const uint8_t* residues, const uint
     }
     std::vector<uint32_t> perm(n);
     for (uint64_t k = 0; k < n; ++k) perm[k] = order[k];
+    ctx->rec_pos.assign(n, 0u);
+    for (uint64_t k = 0; k < n; ++k) ctx->rec_pos[order[k]] = (uint32_t)k;
+    ctx->rec_len = len;
 
     ctx->n_records = (int64_t)n;
     ctx->n_pairs = (int64_t)nonempty;

@@ -41,6 +41,7 @@ inline void dev_free(T*& p) {
 
 struct sw_batch_state;   // batched search buffers and captured graphs (sw_batch.cu)
 struct sw_serve_state;   // serving loop: slots, ring of DB chunks, scheduler (sw_serve.cu)
+struct sw_tb_state;      // traceback scratch (sw_traceback.cu)
 
 struct sw_ctx {
     int device = 0;
@@ -80,6 +81,8 @@ struct sw_ctx {
     uint64_t db_bytes = 0;
     std::vector<uint32_t> pair_ncols;  // host copy, for shape selection
     uint64_t pair_cols_total = 0;      // sum of pair_ncols
+    std::vector<uint32_t> rec_pos;     // record -> sorted position (host)
+    std::vector<uint32_t> rec_len;     // record -> length (host)
     uint4* d_db = nullptr;
     swb::Pair2* d_pairs = nullptr;
     uint32_t* d_perm = nullptr;        // sorted position -> record
@@ -92,6 +95,7 @@ struct sw_ctx {
     int max_cols = 0;                  // longest pair, padded to 8 columns
     sw_batch_state* batch = nullptr;
     sw_serve_state* serve = nullptr;   // non-null between sw_serve_start and sw_serve_stop
+    sw_tb_state* tb = nullptr;
 
     // per-query buffers
     size_t query_cap = 0;
@@ -115,4 +119,6 @@ sw_status take_marks(sw_ctx* ctx, sw_ctx::Marks* m);
 sw_status drain(sw_ctx* ctx, float* last_ms, float* last_fp_ms);
 void free_batch(sw_ctx* ctx);
 void serve_teardown(sw_ctx* ctx);
+void free_traceback(sw_ctx* ctx);
+sw_status ensure_query_buffers(sw_ctx* ctx, size_t qlen);
 }  // namespace swb

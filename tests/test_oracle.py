@@ -123,3 +123,31 @@ def test_blosum62_is_the_reference_table():
     j = src.index("};", i)
     nums = [int(x) for x in re.findall(r"-?\d+", src[i + len("blosum62[32][32] ="):j])]
     np.testing.assert_array_equal(np.array(nums).reshape(32, 32), M)
+
+
+def test_oracle_traceback_is_consistent():
+    """The oracle's traceback reaches the Gotoh score along the path its CIGAR
+    describes, for homologs and random pairs under several gap costs."""
+    import re
+    rng = np.random.default_rng(71)
+    M = param.blosum62()
+    for trial in range(40):
+        q = synth.residues(rng, int(rng.integers(1, 120)))
+        d = synth.residues(rng, int(rng.integers(1, 160)))
+        if trial % 2:
+            d = np.concatenate([d[:20], synth.mutate(rng, q, 0.25, 0.08), d[20:]])
+        oe, e = [(12, 2), (6, 1), (14, 3)][trial % 3]
+        al = oracle.traceback(q, d, M, oe, e)
+        assert al["score"] == oracle.gotoh(q, d, M, oe, e)
+        i, j, s = al["q_begin"], al["d_begin"], 0
+        for n, op in re.findall(r"(\d+)([MID])", al["cigar"]):
+            n = int(n)
+            if op == "M":
+                s += sum(int(M[q[i + k], d[j + k]]) for k in range(n))
+                i += n
+                j += n
+            else:
+                s -= oe + e * (n - 1)
+                i, j = (i + n, j) if op == "I" else (i, j + n)
+        assert (i, j) == (al["q_end"], al["d_end"])
+        assert s == al["score"]
