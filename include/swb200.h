@@ -121,7 +121,8 @@ sw_status sw_ctx_create(int device, const sw_params *params, struct sw_ctx **out
 /* Replaces CUDAWorker::free / ~CUDAWorker. */
 sw_status sw_ctx_destroy(struct sw_ctx *ctx);
 
-/* Text of the last error on this context (never NULL). */
+/* Text of the last error on this context (never NULL).  With ctx NULL: the
+ * last error of a context-free call (the DB image functions) on this thread. */
 const char *sw_last_error(const struct sw_ctx *ctx);
 
 /* ---- database ------------------------------------------------------------ */
@@ -135,6 +136,57 @@ sw_status sw_db_load(struct sw_ctx *ctx, const uint8_t *residues,
                      const uint64_t *offsets, uint64_t n_records);
 
 sw_status sw_db_stats_get(const struct sw_ctx *ctx, sw_db_stats *out);
+
+/* ---- DB image on disk ------------------------------------------------------ */
+
+/* Replaces DBmaker's .seq/.map/.title files (FastaFile::makeDatabase,
+ * src/FastaFile.cpp:182-359, read by DataPool::fill/getTitle,
+ * src/DataPool.cpp:171-310) with one checksummed, mmap-able file: records
+ * in FASTA order (a hit's index is its FASTA position), their offsets, a
+ * title index and the stable longest-first order the device layout uses. */
+typedef struct sw_image_info {
+    uint64_t n_records;
+    uint64_t n_residues;
+    uint64_t file_bytes;
+    uint64_t titles_bytes;
+    uint64_t checksum;      /* 64-bit FNV-1a of everything after the header */
+    uint32_t version;
+    uint32_t reserved;
+} sw_image_info;
+
+/* Writes an image of records held in memory (codes 0..24; titles and
+ * title_offsets (n_records+1) may be NULL for empty titles).  The file is
+ * written under path + ".tmp" and renamed into place. */
+sw_status sw_db_write_image(const char *path, const uint8_t *residues, const uint64_t *offsets,
+                            uint64_t n_records, const char *titles,
+                            const uint64_t *title_offsets);
+
+/* FASTA -> image (replaces DBmaker; FastaFile::nextSeq, src/FastaFile.cpp:
+ * 110-145).  A record is a '>' header line (its title, without the '>') and
+ * the sequence lines up to the next header; letters map as in sw_encode
+ * (either case; '@' = 23; other characters = 24, where the reference's table
+ * gives -1); whitespace, including '\r', is skipped rather than stored.
+ * Sequence text before the first header is SW_ERR_FORMAT.  info may be NULL. */
+sw_status sw_fasta_to_image(const char *fasta_path, const char *image_path,
+                            sw_image_info *info);
+
+/* Checks an image (magic, version, section bounds, offset tables and, when
+ * verify_checksum != 0, the checksum: SW_ERR_FORMAT on any mismatch) and
+ * reports its sizes.  Needs no device. */
+sw_status sw_image_get_info(const char *path, int verify_checksum, sw_image_info *info);
+
+/* sw_db_load from an image: maps the file, checks it as sw_image_get_info
+ * does, builds the device layout from the stored order (checked to be the
+ * stable longest-first permutation) and keeps the file mapped for titles. */
+sw_status sw_db_load_image(struct sw_ctx *ctx, const char *path, int verify_checksum);
+
+/* A record's title from the image the resident DB was loaded from (replaces
+ * DataPool::getTitle, src/DataPool.cpp:289-310).  *title points into the
+ * mapping (not NUL-terminated, *length bytes) and stays valid until the next
+ * sw_db_load* or sw_ctx_destroy.  SW_ERR_STATE when the DB did not come from
+ * an image. */
+sw_status sw_db_title(const struct sw_ctx *ctx, uint64_t record, const char **title,
+                      uint64_t *length);
 
 /* ---- plain search: one query per call ------------------------------------ */
 

@@ -31,7 +31,8 @@ EXPORTS = [
     "sw_set_tuning", "sw_score_noalloc", "sw_get_shapes", "sw_set_batch_options",
     "sw_search_batch", "sw_serve_options_default", "sw_serve_start", "sw_serve_submit",
     "sw_serve_poll", "sw_serve_get_stats", "sw_serve_clock_ms", "sw_serve_stop",
-    "sw_traceback",
+    "sw_traceback", "sw_db_write_image", "sw_fasta_to_image", "sw_image_get_info",
+    "sw_db_load_image", "sw_db_title",
 ]
 
 
@@ -67,6 +68,13 @@ class sw_batch_options(ctypes.Structure):
                 ("long_rows_per_thread", ctypes.c_int32), ("use_graph", ctypes.c_int32),
                 ("group_width", ctypes.c_int32), ("rows_per_thread", ctypes.c_int32),
                 ("stack_rows", ctypes.c_int32)]
+
+
+class sw_image_info(ctypes.Structure):
+    _fields_ = [("n_records", ctypes.c_uint64), ("n_residues", ctypes.c_uint64),
+                ("file_bytes", ctypes.c_uint64), ("titles_bytes", ctypes.c_uint64),
+                ("checksum", ctypes.c_uint64), ("version", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
 
 
 class sw_alignment(ctypes.Structure):
@@ -186,6 +194,18 @@ def load(path: str = LIB_PATH):
     L.sw_score_noalloc.argtypes = [ctypes.c_int, ctypes.POINTER(sw_params), ctypes.c_void_p,
                                    ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                    ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]
+    L.sw_db_write_image.restype = ctypes.c_int
+    L.sw_db_write_image.argtypes = [ctypes.c_char_p, P, P, ctypes.c_uint64, P, P]
+    L.sw_fasta_to_image.restype = ctypes.c_int
+    L.sw_fasta_to_image.argtypes = [ctypes.c_char_p, ctypes.c_char_p,
+                                    ctypes.POINTER(sw_image_info)]
+    L.sw_image_get_info.restype = ctypes.c_int
+    L.sw_image_get_info.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.POINTER(sw_image_info)]
+    L.sw_db_load_image.restype = ctypes.c_int
+    L.sw_db_load_image.argtypes = [P, ctypes.c_char_p, ctypes.c_int]
+    L.sw_db_title.restype = ctypes.c_int
+    L.sw_db_title.argtypes = [P, ctypes.c_uint64, ctypes.POINTER(ctypes.c_void_p),
+                              ctypes.POINTER(ctypes.c_uint64)]
     L.sw_traceback.restype = ctypes.c_int
     L.sw_traceback.argtypes = [P, P, ctypes.c_uint32, P, ctypes.c_uint32,
                                ctypes.POINTER(sw_alignment), P, ctypes.c_uint64,
@@ -208,6 +228,46 @@ def load(path: str = LIB_PATH):
     L.sw_serve_stop.argtypes = [P]
     _lib = L
     return L
+
+
+def _image_call(st: int, what: str):
+    if st != SW_OK:
+        raise SwError(st, f"{what}: {load().sw_last_error(None).decode()}")
+
+
+def _info(i: sw_image_info) -> dict:
+    return dict(n_records=i.n_records, n_residues=i.n_residues, file_bytes=i.file_bytes,
+                titles_bytes=i.titles_bytes, checksum=i.checksum, version=i.version)
+
+
+def write_image(path: str, residues: np.ndarray, offsets: np.ndarray, titles=None):
+    """DB image of records held in memory; titles: list of str or None."""
+    r = np.ascontiguousarray(residues, dtype=np.uint8)
+    o = np.ascontiguousarray(offsets, dtype=np.uint64)
+    t = to = None
+    if titles is not None:
+        enc = [x.encode() for x in titles]
+        t = np.frombuffer(b"".join(enc) or b"\0", dtype=np.uint8).copy()
+        to = np.zeros(len(enc) + 1, dtype=np.uint64)
+        to[1:] = np.cumsum([len(x) for x in enc])
+    _image_call(load().sw_db_write_image(path.encode(), _ptr(r) if r.size else None, _ptr(o),
+                                         len(o) - 1, _ptr(t) if t is not None else None,
+                                         _ptr(to) if to is not None else None),
+                "sw_db_write_image")
+
+
+def fasta_to_image(fasta_path: str, image_path: str) -> dict:
+    i = sw_image_info()
+    _image_call(load().sw_fasta_to_image(fasta_path.encode(), image_path.encode(),
+                                         ctypes.byref(i)), "sw_fasta_to_image")
+    return _info(i)
+
+
+def image_info(path: str, verify: bool = True) -> dict:
+    i = sw_image_info()
+    _image_call(load().sw_image_get_info(path.encode(), 1 if verify else 0, ctypes.byref(i)),
+                "sw_image_get_info")
+    return _info(i)
 
 
 def serve_clock_ms() -> float:
@@ -293,6 +353,18 @@ class Context:
         o = np.ascontiguousarray(offsets, dtype=np.uint64)
         self._check(self.L.sw_db_load(self.h, _ptr(r), _ptr(o), len(o) - 1), "sw_db_load")
         self.n_records = len(o) - 1
+
+    def load_image(self, path: str, verify: bool = True):
+        self._check(self.L.sw_db_load_image(self.h, path.encode(), 1 if verify else 0),
+                    "sw_db_load_image")
+        self.n_records = int(self.db_stats().n_records)
+
+    def title(self, record: int) -> str:
+        p = ctypes.c_void_p()
+        n = ctypes.c_uint64(0)
+        self._check(self.L.sw_db_title(self.h, record, ctypes.byref(p), ctypes.byref(n)),
+                    "sw_db_title")
+        return ctypes.string_at(p.value, n.value).decode(errors="replace") if n.value else ""
 
     def db_stats(self) -> sw_db_stats:
         s = sw_db_stats()

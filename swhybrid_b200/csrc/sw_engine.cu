@@ -138,7 +138,7 @@ extern "C" sw_status sw_encode(const char* letters, uint64_t n, uint8_t* codes) 
 // ---------------------------------------------------------------------------
 
 extern "C" const char* sw_last_error(const sw_ctx* ctx) {
-    return ctx ? ctx->err.c_str() : "null context";
+    return ctx ? ctx->err.c_str() : swb::thread_error();
 }
 
 static sw_status validate_params(sw_ctx* ctx, const sw_params* p) {
@@ -230,6 +230,7 @@ extern "C" sw_status sw_ctx_create(int device, const sw_params* params, sw_ctx**
 static void free_db(sw_ctx* ctx) {
     swb::free_batch(ctx);
     swb::free_traceback(ctx);
+    swb::free_image(ctx);
     ctx->rec_pos.clear();
     ctx->rec_len.clear();
     dev_free(ctx->d_rs_scratch);
@@ -280,6 +281,14 @@ extern "C" sw_status sw_ctx_destroy(sw_ctx* ctx) {
 
 extern "C" sw_status sw_db_load(sw_ctx* ctx, const uint8_t* residues, const uint64_t* offsets,
                                 uint64_t n) {
+    return swb::db_load(ctx, residues, offsets, n, nullptr);
+}
+
+// The layout build behind sw_db_load and sw_db_load_image.  `given_order`
+// (optional) is the length order stored in a DB image: used after checking
+// that it is the stable longest-first permutation.
+sw_status swb::db_load(sw_ctx* ctx, const uint8_t* residues, const uint64_t* offsets, uint64_t n,
+                       const uint32_t* given_order) {
     if (!ctx) return SW_ERR_INVALID;
     if (ctx->serve) return SW_ERR_BUSY;   // the serving loop owns the stream and the DB
     if (!offsets || (n && !residues && offsets[n] != offsets[0]))
@@ -307,9 +316,26 @@ extern "C" sw_status sw_db_load(sw_ctx* ctx, const uint8_t* residues, const uint
                                  base[i], (unsigned long long)i);
     // sort by length (longest first), stable in record order
     std::vector<uint32_t> order(n);
-    std::iota(order.begin(), order.end(), 0u);
-    std::stable_sort(order.begin(), order.end(),
-                     [&](uint32_t a, uint32_t b) { return len[a] > len[b]; });
+    if (given_order) {
+        std::vector<bool> seen(n, false);
+        for (uint64_t k = 0; k < n; ++k) {
+            const uint32_t r = given_order[k];
+            bool ok = r < n && !seen[r];
+            if (ok && k > 0) {
+                const uint32_t p = given_order[k - 1];
+                ok = len[p] > len[r] || (len[p] == len[r] && p < r);
+            }
+            if (!ok) SW_SET(ctx, SW_ERR_FORMAT, "stored length order is not the stable "
+                                               "longest-first permutation (entry %llu)",
+                            (unsigned long long)k);
+            seen[r] = true;
+            order[k] = r;
+        }
+    } else {
+        std::iota(order.begin(), order.end(), 0u);
+        std::stable_sort(order.begin(), order.end(),
+                         [&](uint32_t a, uint32_t b) { return len[a] > len[b]; });
+    }
     const uint64_t npairs_all = (n + 1) / 2;
     std::vector<Pair2> pairs(npairs_all);
     uint64_t units = 0, nonempty = 0;

@@ -96,6 +96,9 @@ struct sw_ctx {
     sw_batch_state* batch = nullptr;
     sw_serve_state* serve = nullptr;   // non-null between sw_serve_start and sw_serve_stop
     sw_tb_state* tb = nullptr;
+    // DB image the resident DB came from (read-only mapping; titles are read from it)
+    const uint8_t* image = nullptr;
+    size_t image_bytes = 0;
 
     // per-query buffers
     size_t query_cap = 0;
@@ -120,5 +123,9 @@ sw_status drain(sw_ctx* ctx, float* last_ms, float* last_fp_ms);
 void free_batch(sw_ctx* ctx);
 void serve_teardown(sw_ctx* ctx);
 void free_traceback(sw_ctx* ctx);
+void free_image(sw_ctx* ctx);
+sw_status db_load(sw_ctx* ctx, const uint8_t* residues, const uint64_t* offsets, uint64_t n,
+                  const uint32_t* given_order);
+const char* thread_error();   // message of this thread's last context-free call
 sw_status ensure_query_buffers(sw_ctx* ctx, size_t qlen);
 }  // namespace swb
