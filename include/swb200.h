@@ -107,6 +107,20 @@ typedef struct sw_run_stats {
 /* BLOSUM62, open 10, extend 2, top 10, reference cap on (Param.h:59-117). */
 void sw_params_default(sw_params *p);
 
+/* The -m option the reference documents (README.md:130) but does not parse
+ * (its Param always uses the BLOSUM62 of Param.h:8-51).  Sets p->matrix from
+ * a matrix in the common text layout: '#' comments, a line of column letters,
+ * then per row its letter and one integer (-127..127) per column.  Letters of
+ * the 23-letter alphabet (either case) are used; others ('*', J, O, U, ...)
+ * are skipped, since those residues always score 0 (code 24), and letters the
+ * text lacks score 0.  SW_ERR_FORMAT on a malformed text; message in
+ * sw_last_error(NULL). */
+sw_status sw_params_parse_matrix(sw_params *p, const char *text);
+
+/* "blosum62" (any case): the built-in table; anything else: a file read with
+ * sw_params_parse_matrix. */
+sw_status sw_params_load_matrix(sw_params *p, const char *name_or_path);
+
 /* Letters to residue codes.  Replaces DataPool::amino_acids_trans
  * (src/DataPool.cpp:33-47) as used by DataPool::getQuery (:312-344) and
  * FastaFile::nextSeq (src/FastaFile.cpp:110-145). */

@@ -32,7 +32,7 @@ EXPORTS = [
     "sw_search_batch", "sw_serve_options_default", "sw_serve_start", "sw_serve_submit",
     "sw_serve_poll", "sw_serve_get_stats", "sw_serve_clock_ms", "sw_serve_stop",
     "sw_traceback", "sw_db_write_image", "sw_fasta_to_image", "sw_image_get_info",
-    "sw_db_load_image", "sw_db_title",
+    "sw_db_load_image", "sw_db_title", "sw_params_parse_matrix", "sw_params_load_matrix",
 ]
 
 
@@ -194,6 +194,10 @@ def load(path: str = LIB_PATH):
     L.sw_score_noalloc.argtypes = [ctypes.c_int, ctypes.POINTER(sw_params), ctypes.c_void_p,
                                    ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                    ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]
+    L.sw_params_parse_matrix.restype = ctypes.c_int
+    L.sw_params_parse_matrix.argtypes = [ctypes.POINTER(sw_params), ctypes.c_char_p]
+    L.sw_params_load_matrix.restype = ctypes.c_int
+    L.sw_params_load_matrix.argtypes = [ctypes.POINTER(sw_params), ctypes.c_char_p]
     L.sw_db_write_image.restype = ctypes.c_int
     L.sw_db_write_image.argtypes = [ctypes.c_char_p, P, P, ctypes.c_uint64, P, P]
     L.sw_fasta_to_image.restype = ctypes.c_int
@@ -228,6 +232,24 @@ def load(path: str = LIB_PATH):
     L.sw_serve_stop.argtypes = [P]
     _lib = L
     return L
+
+
+def parse_matrix(text: str) -> np.ndarray:
+    """32x32 scoring matrix (search codes) from substitution-matrix text."""
+    p = sw_params()
+    load().sw_params_default(ctypes.byref(p))
+    _image_call(load().sw_params_parse_matrix(ctypes.byref(p), text.encode()),
+                "sw_params_parse_matrix")
+    return np.array(p.matrix[:], dtype=np.int32).reshape(32, 32)
+
+
+def load_matrix(name_or_path: str) -> np.ndarray:
+    """'blosum62' or a matrix file, as a 32x32 array (search codes)."""
+    p = sw_params()
+    load().sw_params_default(ctypes.byref(p))
+    _image_call(load().sw_params_load_matrix(ctypes.byref(p), name_or_path.encode()),
+                "sw_params_load_matrix")
+    return np.array(p.matrix[:], dtype=np.int32).reshape(32, 32)
 
 
 def _image_call(st: int, what: str):

@@ -44,6 +44,16 @@ public:
                 case 't': topNum = std::atoi(argv[++i]); break;
                 case 'g': cudaNum = std::atoi(argv[++i]); break;
                 case 'q': queryPath = argv[++i]; break;
+                case 'm': {   // scoring matrix: "blosum62" or a matrix file
+                    if (sw_params_load_matrix(&p, argv[++i]) != SW_OK)
+                        throw std::invalid_argument(std::string("-m: ") + sw_last_error(nullptr));
+                    for (int r = 0; r < 32; ++r)
+                        for (int c = 0; c < 32; ++c) {
+                            matrix[r][c] = p.matrix[r * 32 + c];
+                            plain_matrix[r * 32 + c] = p.matrix[r * 32 + c];
+                        }
+                    break;
+                }
                 case 'd':
                     if (argv[i][2] == 'b') dbPath = argv[++i];
                     break;

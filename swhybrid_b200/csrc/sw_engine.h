@@ -127,5 +127,6 @@ void free_image(sw_ctx* ctx);
 sw_status db_load(sw_ctx* ctx, const uint8_t* residues, const uint64_t* offsets, uint64_t n,
                   const uint32_t* given_order);
 const char* thread_error();   // message of this thread's last context-free call
+sw_status thread_fail(sw_status st, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
 sw_status ensure_query_buffers(sw_ctx* ctx, size_t qlen);
 }  // namespace swb

@@ -56,18 +56,7 @@ struct ImageHeader {
 };
 static_assert(sizeof(ImageHeader) == 128, "image header");
 
-thread_local std::string t_err;
-
-sw_status fail(sw_status st, const char* fmt, ...) __attribute__((format(printf, 2, 3)));
-sw_status fail(sw_status st, const char* fmt, ...) {
-    char b[512];
-    va_list ap;
-    va_start(ap, fmt);
-    vsnprintf(b, sizeof(b), fmt, ap);
-    va_end(ap);
-    t_err = b;
-    return st;
-}
+using swb::thread_fail;
 
 uint64_t align64(uint64_t x) { return (x + 63) & ~uint64_t(63); }
 
@@ -128,28 +117,28 @@ struct Writer {
 // (empty titles).
 sw_status write_image(const char* path, const uint8_t* residues, const uint64_t* offsets,
                       uint64_t n, const char* titles, const uint64_t* title_offsets) {
-    if (!path || (n && !offsets)) return fail(SW_ERR_INVALID, "null argument");
+    if (!path || (n && !offsets)) return thread_fail(SW_ERR_INVALID, "null argument");
     uint64_t total = 0;
     std::vector<uint32_t> len(n);
     for (uint64_t i = 0; i < n; ++i) {
-        if (offsets[i + 1] < offsets[i]) return fail(SW_ERR_INVALID, "offsets not monotone at %llu",
+        if (offsets[i + 1] < offsets[i]) return thread_fail(SW_ERR_INVALID, "offsets not monotone at %llu",
                                                      (unsigned long long)i);
         len[i] = (uint32_t)(offsets[i + 1] - offsets[i]);
         total += len[i];
     }
-    if (total && !residues) return fail(SW_ERR_INVALID, "null residues");
+    if (total && !residues) return thread_fail(SW_ERR_INVALID, "null residues");
     const uint8_t* base = n ? residues + offsets[0] : residues;
     for (uint64_t i = 0; i < total; ++i)
-        if (base[i] > 24) return fail(SW_ERR_INVALID, "residue code %d at %llu", base[i],
+        if (base[i] > 24) return thread_fail(SW_ERR_INVALID, "residue code %d at %llu", base[i],
                                       (unsigned long long)i);
     uint64_t tbytes = 0;
     if (title_offsets) {
         for (uint64_t i = 0; i < n; ++i)
             if (title_offsets[i + 1] < title_offsets[i])
-                return fail(SW_ERR_INVALID, "title offsets not monotone at %llu",
+                return thread_fail(SW_ERR_INVALID, "title offsets not monotone at %llu",
                             (unsigned long long)i);
         tbytes = n ? title_offsets[n] - title_offsets[0] : 0;
-        if (tbytes && !titles) return fail(SW_ERR_INVALID, "null titles");
+        if (tbytes && !titles) return thread_fail(SW_ERR_INVALID, "null titles");
     }
     std::vector<uint32_t> order(n);
     std::iota(order.begin(), order.end(), 0u);
@@ -171,7 +160,7 @@ sw_status write_image(const char* path, const uint8_t* residues, const uint64_t*
     const std::string tmp = std::string(path) + ".tmp";
     Writer w;
     w.f = fopen(tmp.c_str(), "wb");
-    if (!w.f) return fail(SW_ERR_INVALID, "cannot create %s", tmp.c_str());
+    if (!w.f) return thread_fail(SW_ERR_INVALID, "cannot create %s", tmp.c_str());
     bool ok = fwrite(&h, sizeof(h), 1, w.f) == 1;
     w.pos = sizeof(h);
     std::vector<uint64_t> o(n + 1, 0);
@@ -188,11 +177,11 @@ sw_status write_image(const char* path, const uint8_t* residues, const uint64_t*
     ok = (fclose(w.f) == 0) && ok;
     if (!ok) {
         unlink(tmp.c_str());
-        return fail(SW_ERR_INVALID, "write to %s failed", tmp.c_str());
+        return thread_fail(SW_ERR_INVALID, "write to %s failed", tmp.c_str());
     }
     if (rename(tmp.c_str(), path) != 0) {
         unlink(tmp.c_str());
-        return fail(SW_ERR_INVALID, "cannot rename %s to %s", tmp.c_str(), path);
+        return thread_fail(SW_ERR_INVALID, "cannot rename %s to %s", tmp.c_str(), path);
     }
     return SW_OK;
 }
@@ -210,24 +199,24 @@ struct Mapped {
 };
 
 sw_status map_image(const char* path, bool verify_checksum, Mapped* m) {
-    if (!path) return fail(SW_ERR_INVALID, "null path");
+    if (!path) return thread_fail(SW_ERR_INVALID, "null path");
     const int fd = open(path, O_RDONLY);
-    if (fd < 0) return fail(SW_ERR_INVALID, "cannot open %s", path);
+    if (fd < 0) return thread_fail(SW_ERR_INVALID, "cannot open %s", path);
     struct stat st;
     if (fstat(fd, &st) != 0 || st.st_size < (off_t)sizeof(ImageHeader)) {
         close(fd);
-        return fail(SW_ERR_FORMAT, "%s: too short for a DB image", path);
+        return thread_fail(SW_ERR_FORMAT, "%s: too short for a DB image", path);
     }
     void* p = mmap(nullptr, (size_t)st.st_size, PROT_READ, MAP_PRIVATE, fd, 0);
     close(fd);
-    if (p == MAP_FAILED) return fail(SW_ERR_INVALID, "cannot map %s", path);
+    if (p == MAP_FAILED) return thread_fail(SW_ERR_INVALID, "cannot map %s", path);
     m->base = (const uint8_t*)p;
     m->bytes = (size_t)st.st_size;
     m->h = (const ImageHeader*)p;
     const ImageHeader& h = *m->h;
     auto bad = [&](const char* what) {
         m->release();
-        return fail(SW_ERR_FORMAT, "%s: %s", path, what);
+        return thread_fail(SW_ERR_FORMAT, "%s: %s", path, what);
     };
     if (memcmp(h.magic, kMagic, 8) != 0) return bad("not a DB image (magic)");
     if (h.version != kImageVersion) return bad("unsupported image version");
@@ -279,7 +268,21 @@ struct Alphabet {
 
 namespace swb {
 
+namespace {
+thread_local std::string t_err;
+}
+
 const char* thread_error() { return t_err.c_str(); }
+
+sw_status thread_fail(sw_status st, const char* fmt, ...) {
+    char b[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(b, sizeof(b), fmt, ap);
+    va_end(ap);
+    t_err = b;
+    return st;
+}
 
 void free_image(sw_ctx* ctx) {
     if (ctx->image) munmap((void*)ctx->image, ctx->image_bytes);
@@ -297,9 +300,9 @@ extern "C" sw_status sw_db_write_image(const char* path, const uint8_t* residues
 
 extern "C" sw_status sw_fasta_to_image(const char* fasta_path, const char* image_path,
                                        sw_image_info* info) {
-    if (!fasta_path || !image_path) return fail(SW_ERR_INVALID, "null path");
+    if (!fasta_path || !image_path) return thread_fail(SW_ERR_INVALID, "null path");
     FILE* f = fopen(fasta_path, "rb");
-    if (!f) return fail(SW_ERR_INVALID, "cannot open %s", fasta_path);
+    if (!f) return thread_fail(SW_ERR_INVALID, "cannot open %s", fasta_path);
     static const Alphabet A;
     std::vector<uint8_t> res;
     std::vector<uint64_t> off{0};
@@ -341,7 +344,7 @@ extern "C" sw_status sw_fasta_to_image(const char* fasta_path, const char* image
             if (A.skip[(uint8_t)c]) continue;
             if (!any) {
                 fclose(f);
-                return fail(SW_ERR_FORMAT, "%s line %llu: sequence before the first '>' header",
+                return thread_fail(SW_ERR_FORMAT, "%s line %llu: sequence before the first '>' header",
                             fasta_path, (unsigned long long)line);
             }
             res.push_back(A.code[(uint8_t)c]);
@@ -349,7 +352,7 @@ extern "C" sw_status sw_fasta_to_image(const char* fasta_path, const char* image
     }
     const bool read_error = ferror(f) != 0;
     fclose(f);
-    if (read_error) return fail(SW_ERR_INVALID, "read error in %s", fasta_path);
+    if (read_error) return thread_fail(SW_ERR_INVALID, "read error in %s", fasta_path);
     if (any) {
         off.push_back(res.size());
         toff.push_back(titles.size());
@@ -363,7 +366,7 @@ extern "C" sw_status sw_fasta_to_image(const char* fasta_path, const char* image
 
 extern "C" sw_status sw_image_get_info(const char* path, int verify_checksum,
                                        sw_image_info* info) {
-    if (!info) return fail(SW_ERR_INVALID, "null argument");
+    if (!info) return thread_fail(SW_ERR_INVALID, "null argument");
     Mapped m;
     sw_status st = map_image(path, verify_checksum != 0, &m);
     if (st != SW_OK) return st;
