@@ -1,0 +1,79 @@
+"""Sharded search on two ranks (gloo, CPU): the residue-balanced split, the
+local-to-global index mapping and the k-hit all-gather merge must give the
+whole-DB top-k, ties across the shard boundary included.  The oracle stands
+in for each rank's device search (no GPU here)."""
+import os
+import socket
+
+import numpy as np
+import torch.distributed as dist
+import torch.multiprocessing as mp
+
+import oracle
+from swhybrid_b200 import param, shard, synth
+
+K = 10
+
+
+def make_case():
+    rng = np.random.default_rng(91)
+    db = synth.small_db(92, 900)
+    q = synth.residues(rng, 120)
+    recs = [db.record(i) for i in range(db.n)]
+    # the same homolog at both ends of the DB: equal scores on both shards
+    h = synth.mutate(rng, q, 0.15, 0.0)
+    for i in (3, 7, db.n - 5, db.n - 2):
+        recs[i] = h
+    lens = np.array([len(r) for r in recs], dtype=np.int64)
+    off = np.zeros(db.n + 1, dtype=np.uint64)
+    off[1:] = np.cumsum(lens)
+    return np.concatenate(recs).astype(np.uint8), off, q
+
+
+def worker(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        res, off, q = make_case()
+        b, e = shard.shard_bounds(off, world)[rank]
+        lres, loff = shard.local_records(res, off, b, e)
+        scores = oracle.search(q, lres, loff, param.blosum62(), 12, 2)
+        sc, idx = oracle.topk(scores, K)
+        merged = shard.gather_topk(list(zip(sc.tolist(), idx.tolist())), b, K)
+        out[rank] = merged
+    finally:
+        dist.destroy_process_group()
+
+
+def free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def test_two_rank_merge_equals_whole_db():
+    world = 2
+    with mp.Manager() as m:
+        out = m.dict()
+        mp.spawn(worker, args=(world, free_port(), out), nprocs=world, join=True)
+        got = dict(out)
+    res, off, q = make_case()
+    sc, idx = oracle.topk(oracle.search(q, res, off, param.blosum62(), 12, 2), K)
+    want = list(zip(sc.tolist(), idx.tolist()))
+    assert got[0] == want and got[1] == want
+    assert want[0][0] == want[3][0]            # the planted ties made it into the list
+
+
+def test_shard_bounds_balance_and_cover():
+    rng = np.random.default_rng(3)
+    lens = rng.integers(0, 2000, size=1000)
+    off = np.zeros(1001, dtype=np.int64)
+    off[1:] = np.cumsum(lens)
+    for world in (1, 2, 3, 8):
+        b = shard.shard_bounds(off, world)
+        assert b[0][0] == 0 and b[-1][1] == 1000
+        assert all(b[i][1] == b[i + 1][0] for i in range(world - 1))
+        sizes = [int(off[e] - off[s]) for s, e in b]
+        assert max(sizes) - min(sizes) <= 2 * int(lens.max())
+    assert shard.shard_bounds(np.zeros(1, dtype=np.int64), 4) == [(0, 0)] * 4
