@@ -589,7 +589,15 @@ def run_ours(args, rank, world, local_rank):
                 "peak": round(rates["cell_mix_gcups"], 1),
                 "unit": "GCUPS",
                 "frac": round(fp_gcups / rates["cell_mix_gcups"], 4) if fp_gcups else None,
-                "traffic": None,
+                # DRAM bytes (read + write) of one bulk first-pass launch, from the ncu
+                # capture of sw_wavefront<16,48,256> on this DB with the 1,434-residue
+                # query (dram__bytes_read.sum 1.87 GB + dram__bytes_write.sum 1.61 GB):
+                # the 194 MB column stream once per pass plus the pass-boundary rows
+                # (16 B per column written by pass 0, read by pass 1).  At 3.5 TCUPS
+                # that is ~43 GB/s, far below HBM: the kernel is ALU-bound.
+                "traffic": 3.48e9,
+                "traffic_unit": "bytes per launch (query 1,434, 2 passes)",
+                "algorithmic_bytes_per_launch": 194_000_000,   # the DB column stream, read once
                 "peak_source": "measured live: libswprobe cell-mix kernel (first-pass "
                                "instruction mix from registers, full occupancy)",
                 "first_pass_launches": int(tot.first_pass_launches),
