@@ -286,11 +286,19 @@ typedef struct sw_batch_options {
     int32_t group_width;
     int32_t rows_per_thread;
     int32_t stack_rows;
+    int32_t pair_rows;      /* queries of at most this many residues are scored two per
+                               register (pair_group_width x pair_rows_per_thread); 0 = off */
+    int32_t pair_group_width;
+    int32_t pair_rows_per_thread;
 } sw_batch_options;
 
 /* NULL restores the defaults (no cut-over, long shape 32x16, graphs on,
  * stacks of up to 4096 rows with shape 16x64 -- the best measured on B200
- * for a 64-query batch of lengths 50..5,000 against a 205 M-residue DB). */
+ * for a 64-query batch of lengths 50..5,000 against a 205 M-residue DB --
+ * and queries up to 2048 residues paired two per register with shape 16x64).
+ * Paired queries: two stacks of short queries share every register, one in
+ * each 16-bit lane, against one record, with a pre-packed profile (no
+ * per-row byte unpacking); a lane stack holds at most pair_rows rows. */
 sw_status sw_set_batch_options(struct sw_ctx *ctx, const sw_batch_options *opt);
 
 /* Searches n_queries queries (codes back to back; query_offsets has

@@ -31,11 +31,13 @@
 #include "sw_aux.h"
 #include "sw_device.cuh"
 #include "sw_engine.h"
+#include "sw_qpair.cuh"
 #include "sw_registry.h"
 
 using namespace swb;
 
 struct BatchLaunch {
+    const QpKernel* qk = nullptr;   // set: a paired-query launch over double stacks
     const WfKernel* k;
     int grid, threads;
     size_t smem;
@@ -48,10 +50,22 @@ struct BatchLaunch {
 
 // Host image of a batch's stacks (uploaded as one block, see enqueue_batch).
 struct StackPlan {
-    std::vector<uint8_t> codes;           // stack rows
+    std::vector<uint8_t> codes;           // stack rows (and the paired lanes' rows)
     std::vector<uint32_t> off, rows, rb_off;
     std::vector<int32_t> rb_map;
+    // double stacks of the paired-query kernel: per double stack the two lanes'
+    // codes offset and rows, and per (pass, thread) the (low, high) block map
+    std::vector<uint32_t> qp_off_lo, qp_rows_lo, qp_off_hi, qp_rows_hi, qp_rb_off;
+    std::vector<int32_t> qp_rb_map;       // pairs of entries
 };
+
+const QpKernel* find_qp(int T, int R) {
+    int n = 0;
+    const QpKernel* q = qp_kernels(&n);
+    for (int i = 0; i < n; ++i)
+        if (q[i].T == T && q[i].R == R) return &q[i];
+    return nullptr;
+}
 
 struct BatchGraph {
     cudaGraph_t graph = nullptr;
@@ -60,7 +74,7 @@ struct BatchGraph {
 };
 
 struct sw_batch_state {
-    sw_batch_options opt{0, 32, 16, 1, 16, 64, 4096};
+    sw_batch_options opt{0, 32, 16, 1, 16, 64, 4096, 2048, 16, 64};
     // device
     uint8_t* d_queries = nullptr;
     size_t queries_cap = 0;
@@ -135,20 +149,32 @@ double wall_ms() {
 //   stack_off[ns], stack_rows[ns], rb_off[ns]   uint32
 //   rb_map[...]                                 int32
 //   stack codes                                 uint8
+//   qp_off_lo, qp_rows_lo, qp_off_hi, qp_rows_hi, qp_rb_off [nqp]  uint32
+//   qp_rb_map[...] (16-byte aligned)            int2
 struct MetaLayout {
-    size_t qoff, qlen, soff, srows, rboff, rbmap, codes, total;
+    size_t qoff, qlen, soff, srows, rboff, rbmap, qp_off_lo, qp_rows_lo, qp_off_hi, qp_rows_hi,
+        qp_rboff, qp_rbmap, codes, total;
+    int nst, nqp;
 };
 
 MetaLayout meta_layout(uint32_t nq, const StackPlan& sp) {
     MetaLayout m;
-    const size_t ns = sp.off.size();
+    const size_t ns = sp.off.size(), nqp = sp.qp_off_lo.size();
+    m.nst = (int)ns;
+    m.nqp = (int)nqp;
     m.qoff = 0;
     m.qlen = m.qoff + 4 * (size_t)nq;
     m.soff = m.qlen + 4 * (size_t)nq;
     m.srows = m.soff + 4 * ns;
     m.rboff = m.srows + 4 * ns;
     m.rbmap = m.rboff + 4 * ns;
-    m.codes = m.rbmap + 4 * sp.rb_map.size();
+    m.qp_off_lo = m.rbmap + 4 * sp.rb_map.size();
+    m.qp_rows_lo = m.qp_off_lo + 4 * nqp;
+    m.qp_off_hi = m.qp_rows_lo + 4 * nqp;
+    m.qp_rows_hi = m.qp_off_hi + 4 * nqp;
+    m.qp_rboff = m.qp_rows_hi + 4 * nqp;
+    m.qp_rbmap = (m.qp_rboff + 4 * nqp + 15) / 16 * 16;
+    m.codes = m.qp_rbmap + 4 * sp.qp_rb_map.size();
     m.total = (m.codes + sp.codes.size() + 15) / 16 * 16;
     return m;
 }
@@ -165,8 +191,9 @@ sw_status enqueue_batch(sw_ctx* ctx, sw_batch_state* b, uint32_t nq, size_t qbyt
     const size_t meta_at = (b->stage_cap - ml.total) & ~(size_t)15;
     SW_CUDA(ctx, cudaMemcpyAsync(b->d_meta, b->h_stage + meta_at, ml.total,
                                  cudaMemcpyHostToDevice, st));
-    const int nst = (int)((ml.rboff - ml.srows) / 4);
-    SW_CUDA(ctx, cudaMemsetAsync(b->d_counters, 0, (2 * (size_t)nst + 1) * sizeof(int), st));
+    const int nst = ml.nst;
+    SW_CUDA(ctx, cudaMemsetAsync(b->d_counters, 0, (2 * (size_t)nst + 1 + ml.nqp) * sizeof(int),
+                                 st));
     SW_CUDA(ctx, cudaMemsetAsync(b->d_scores, 0, (size_t)nq * n_rec * sizeof(int), st));
     const uint32_t* d_qoff = reinterpret_cast<const uint32_t*>(b->d_meta + ml.qoff);
     const uint32_t* d_qlen = reinterpret_cast<const uint32_t*>(b->d_meta + ml.qlen);
@@ -179,6 +206,42 @@ sw_status enqueue_batch(sw_ctx* ctx, sw_batch_state* b, uint32_t nq, size_t qbyt
     const int ovf_thresh = 32767 - std::max(ctx->max_score, 1) + 1;
     bool forked = false;
     for (const BatchLaunch& L : launches) {
+        if (L.qk) {      // paired queries: main stream, the bulk half of the boundary rows
+            QpArgs q;
+            q.db = ctx->d_db;
+            q.pairs = ctx->d_pairs;
+            q.pair_begin = 0;
+            q.pair_count = (int)ctx->n_pairs;
+            q.codes = d_codes;
+            q.off_lo = reinterpret_cast<const uint32_t*>(b->d_meta + ml.qp_off_lo) + L.sbegin;
+            q.rows_lo = reinterpret_cast<const uint32_t*>(b->d_meta + ml.qp_rows_lo) + L.sbegin;
+            q.off_hi = reinterpret_cast<const uint32_t*>(b->d_meta + ml.qp_off_hi) + L.sbegin;
+            q.rows_hi = reinterpret_cast<const uint32_t*>(b->d_meta + ml.qp_rows_hi) + L.sbegin;
+            q.rb_map = reinterpret_cast<const int2*>(b->d_meta + ml.qp_rbmap);
+            q.rb_off = reinterpret_cast<const uint32_t*>(b->d_meta + ml.qp_rboff) + L.sbegin;
+            q.nstacks = L.scount;
+            q.counters = b->d_counters + L.counter_base;
+            q.mat = ctx->d_mat;
+            q.bias2 = (uint32_t)(ctx->params.gap_open + ctx->params.gap_extend);
+            q.bias2 |= q.bias2 << 16;
+            q.neg_e = (uint32_t)(uint16_t)(int16_t)(-ctx->params.gap_extend);
+            q.neg_e |= q.neg_e << 16;
+            q.one = 1u;
+            q.bnd = b->d_bnd + b->bnd_cap / 2;
+            q.bnd_group = L.bnd_group;
+            q.scores = b->d_scores;
+            q.n_records = n_rec;
+            q.ovf_list = b->d_ovf;
+            q.ovf_count = d_ovf_count;
+            q.ovf_thresh = ovf_thresh;
+            q.ovf_cap = (int)std::min<size_t>(b->ovf_cap, (size_t)INT32_MAX);
+            q.pair_ids = nullptr;
+            void* args[] = {&q};
+            SW_CUDA(ctx, cudaLaunchKernel(L.qk->fn, dim3((unsigned)L.grid), dim3(L.threads), args,
+                                          L.smem, st));
+            ++*n_launch;
+            continue;
+        }
         BatchArgs a;
         a.db = ctx->d_db;
         a.pairs = ctx->d_pairs;
@@ -295,11 +358,13 @@ extern "C" sw_status sw_set_batch_options(sw_ctx* ctx, const sw_batch_options* o
     if (!ctx->batch) ctx->batch = new sw_batch_state();
     if (opt) {
         if (opt->cutover < 0 || !find_kernel(opt->long_group_width, opt->long_rows_per_thread) ||
-            !find_kernel(opt->group_width, opt->rows_per_thread) || opt->stack_rows < 0)
+            !find_kernel(opt->group_width, opt->rows_per_thread) || opt->stack_rows < 0 ||
+            opt->pair_rows < 0 ||
+            (opt->pair_rows > 0 && !find_qp(opt->pair_group_width, opt->pair_rows_per_thread)))
             SW_SET(ctx, SW_ERR_INVALID, "bad batch options");
         ctx->batch->opt = *opt;
     } else {
-        ctx->batch->opt = sw_batch_options{0, 32, 16, 1, 16, 64, 4096};
+        ctx->batch->opt = sw_batch_options{0, 32, 16, 1, 16, 64, 4096, 2048, 16, 64};
     }
     for (auto& kv : ctx->batch->graphs) {
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
@@ -378,9 +443,16 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
         buckets.back().stacks.push_back(st1);
         ++i0;
     }
-    if (i0 < nz) {
+    // queries of at most pair_rows residues: paired-query double stacks (below)
+    const QpKernel* qk = b->opt.pair_rows > 0
+                             ? find_qp(b->opt.pair_group_width, b->opt.pair_rows_per_thread)
+                             : nullptr;
+    uint32_t ip = nz;
+    if (qk)
+        while (ip > i0 && qlen[order[ip - 1]] <= (uint32_t)b->opt.pair_rows) --ip;
+    if (i0 < ip) {
         Bucket bk{sT, sR, {}};
-        for (uint32_t i = i0; i < nz; ++i) {
+        for (uint32_t i = i0; i < ip; ++i) {
             const uint32_t q = order[i];
             const uint32_t need = (qlen[q] + sR - 1) / sR * sR;
             bool placed = false;
@@ -475,7 +547,86 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
             launches.push_back(L);
         }
     }
-    // counters: bulk of stack i at [i], long at [nst_total + i], overflow count last
+    // paired queries: lanes of at most pair_rows rows (first fit, longest
+    // first, each query padded to whole R-row blocks), consecutive lanes
+    // paired into double stacks, all in one launch
+    if (qk && ip < nz) {
+        const uint32_t qR = (uint32_t)qk->R, qT = (uint32_t)qk->T;
+        const uint32_t lane_cap = std::max<uint32_t>((uint32_t)b->opt.pair_rows, qR);
+        struct Lane {
+            std::vector<uint32_t> q;
+            uint32_t rows = 0;
+        };
+        std::vector<Lane> lanes;
+        for (uint32_t i = ip; i < nz; ++i) {
+            const uint32_t q = order[i];
+            const uint32_t need = (qlen[q] + qR - 1) / qR * qR;
+            bool placed = false;
+            for (Lane& ln : lanes)
+                if (ln.rows + need <= lane_cap) {
+                    ln.q.push_back(q);
+                    ln.rows += need;
+                    placed = true;
+                    break;
+                }
+            if (!placed) lanes.push_back(Lane{{q}, need});
+        }
+        if (lanes.size() % 2) lanes.push_back(Lane{});      // an empty high lane
+        uint32_t max_rows = 0;
+        for (size_t d = 0; d < lanes.size(); d += 2) {
+            const Lane* pair_l[2] = {&lanes[d], &lanes[d + 1]};
+            std::vector<int32_t> blocks[2];
+            for (int h = 0; h < 2; ++h) {
+                const Lane& ln = *pair_l[h];
+                (h ? sp.qp_off_hi : sp.qp_off_lo).push_back((uint32_t)sp.codes.size());
+                (h ? sp.qp_rows_hi : sp.qp_rows_lo).push_back(ln.rows);
+                for (const uint32_t q : ln.q) {
+                    const uint8_t* src = queries + qoffsets[q];
+                    const uint32_t L = qlen[q];
+                    const uint32_t padded = (L + qR - 1) / qR * qR;
+                    sp.codes.insert(sp.codes.end(), src, src + L);
+                    sp.codes.insert(sp.codes.end(), padded - L, (uint8_t)kZeroCode);
+                    for (uint32_t j = 0; j < padded / qR; ++j)
+                        blocks[h].push_back((int32_t)q | (j == 0 ? kFirstBit : 0));
+                }
+            }
+            const uint32_t rows = std::max(lanes[d].rows, lanes[d + 1].rows);
+            max_rows = std::max(max_rows, rows);
+            const uint32_t P = (rows + qT * qR - 1) / (qT * qR);
+            sp.qp_rb_off.push_back((uint32_t)(sp.qp_rb_map.size() / 2));
+            for (uint32_t j = 0; j < P * qT; ++j) {
+                sp.qp_rb_map.push_back(j < blocks[0].size() ? blocks[0][j] : -1);
+                sp.qp_rb_map.push_back(j < blocks[1].size() ? blocks[1][j] : -1);
+            }
+        }
+        const size_t smem = qk->smem((int)max_rows);
+        int occ = 0;
+        if (smem <= (size_t)ctx->max_smem &&
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, qk->fn, qk->block, smem) != cudaSuccess) {
+            cudaGetLastError();
+            occ = 0;
+        }
+        if (occ == 0)
+            SW_SET(ctx, SW_ERR_UNSUPPORTED, "paired lanes of %u rows do not fit shape %dx%d",
+                   max_rows, qk->T, qk->R);
+        BatchLaunch L;
+        L.qk = qk;
+        L.k = nullptr;
+        L.threads = qk->block;
+        L.grid = occ * ctx->num_sms;
+        L.smem = smem;
+        L.sbegin = 0;
+        L.scount = (int)sp.qp_off_lo.size();
+        L.pair_begin = 0;
+        L.pair_count = (int)ctx->n_pairs;
+        L.counter_base = 2 * nst_total + 1;
+        L.long_part = false;
+        L.bnd_group = 2 * (size_t)ctx->max_cols;
+        bnd_bulk = std::max(bnd_bulk, (size_t)L.grid * (L.threads / qk->T) * L.bnd_group);
+        launches.push_back(L);
+    }
+    // counters: bulk of stack i at [i], long at [nst_total + i], overflow count
+    // at [2 nst_total], paired double stack j at [2 nst_total + 1 + j]
     const MetaLayout ml = meta_layout(nq, sp);
 
     // ---- buffers (before any capture) ----
@@ -488,12 +639,13 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
         }
         b->graphs.clear();
     };
+    const size_t counters_need = 2 * (size_t)nst_total + 1 + ml.nqp;
     if (std::max<uint64_t>(qbytes, 1) > b->queries_cap || ml.total > b->meta_cap ||
-        2 * (size_t)nst_total + 1 > b->counters_cap)
+        counters_need > b->counters_cap)
         drop_graphs();
     if ((s = grow(ctx, &b->d_queries, b->queries_cap, std::max<uint64_t>(qbytes, 1), "queries")) != SW_OK) return s;
     if ((s = grow(ctx, &b->d_meta, b->meta_cap, ml.total, "stack table")) != SW_OK) return s;
-    if ((s = grow(ctx, &b->d_counters, b->counters_cap, 2 * (size_t)nst_total + 1, "counters")) != SW_OK) return s;
+    if ((s = grow(ctx, &b->d_counters, b->counters_cap, counters_need, "counters")) != SW_OK) return s;
     if (nq > b->scores_cap) {
         drop_graphs();
         dev_free(b->d_scores);
@@ -563,6 +715,13 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
         memcpy(m + ml.srows, sp.rows.data(), 4 * ns);
         memcpy(m + ml.rboff, sp.rb_off.data(), 4 * ns);
         memcpy(m + ml.rbmap, sp.rb_map.data(), 4 * sp.rb_map.size());
+        const size_t nqp = sp.qp_off_lo.size();
+        memcpy(m + ml.qp_off_lo, sp.qp_off_lo.data(), 4 * nqp);
+        memcpy(m + ml.qp_rows_lo, sp.qp_rows_lo.data(), 4 * nqp);
+        memcpy(m + ml.qp_off_hi, sp.qp_off_hi.data(), 4 * nqp);
+        memcpy(m + ml.qp_rows_hi, sp.qp_rows_hi.data(), 4 * nqp);
+        memcpy(m + ml.qp_rboff, sp.qp_rb_off.data(), 4 * nqp);
+        memcpy(m + ml.qp_rbmap, sp.qp_rb_map.data(), 4 * sp.qp_rb_map.size());
         memcpy(m + ml.codes, sp.codes.data(), sp.codes.size());
     }
 
@@ -574,6 +733,8 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
     sig.push_back((uint64_t)b->opt.cutover);
     sig.push_back((uint64_t)b->opt.group_width << 32 | (uint32_t)b->opt.rows_per_thread);
     sig.push_back((uint64_t)b->opt.stack_rows);
+    sig.push_back((uint64_t)b->opt.pair_rows << 32 |
+                  (uint64_t)(b->opt.pair_group_width * 256 + b->opt.pair_rows_per_thread));
     for (uint32_t i = 0; i < nq; ++i) sig.push_back(qlen[i]);
     uint32_t n_launch = 0;
     SW_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));

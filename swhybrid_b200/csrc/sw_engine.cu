@@ -214,6 +214,11 @@ extern "C" sw_status sw_ctx_create(int device, const sw_params* params, sw_ctx**
             cudaFuncSetAttribute(ks[i].batch_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  ctx->max_smem) != cudaSuccess)
             return fail(SW_ERR_CUDA);
+    const QpKernel* qks = qp_kernels(&nk);
+    for (int i = 0; i < nk; ++i)
+        if (cudaFuncSetAttribute(qks[i].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 ctx->max_smem) != cudaSuccess)
+            return fail(SW_ERR_CUDA);
     // the long-pair kernels also hold a few static shared words
     const LongKernel* lks = long_kernels(&nk);
     for (int i = 0; i < nk; ++i) {

@@ -16,4 +16,12 @@ struct WfKernel {
 // All instantiated shapes (sw_wf_t*.cu).
 const WfKernel* wf_kernels(int* n);
 
+// Paired-query batched kernel shapes (sw_qp.cu).
+struct QpKernel {
+    int T, R, block;
+    const void* fn;                // __global__ sw_qpbatch<T, R, block>
+    size_t (*smem)(int rows);      // shared memory for a double stack of `rows` rows
+};
+const QpKernel* qp_kernels(int* n);
+
 }  // namespace swb

@@ -89,9 +89,9 @@ def test_many_short_queries_share_stacks(ctx):
     db = synth.small_db(14, 2500)
     db, _ = synth.plant_homologs(rng, db, qs[0], 0.01)
     ctx.load_db(db.residues, db.offsets)
-    for opts in ({}, {"stack_shape": (16, 8), "stack_rows": 256},
-                 {"stack_shape": (32, 4), "stack_rows": 4096, "cutover": 200},
-                 {"stack_shape": (16, 32), "stack_rows": 1024, "cutover": 1000}):
+    for opts in ({}, {"stack_shape": (16, 8), "stack_rows": 256, "pair_rows": 0},
+                 {"stack_shape": (32, 4), "stack_rows": 4096, "cutover": 200, "pair_rows": 0},
+                 {"stack_shape": (16, 32), "stack_rows": 1024, "cutover": 1000, "pair_rows": 0}):
         ctx.set_batch_options(**opts)
         try:
             hits, scores = ctx.search_batch(qs, want_scores=True)
@@ -102,3 +102,57 @@ def test_many_short_queries_share_stacks(ctx):
             np.testing.assert_array_equal(scores[qi], want, err_msg=f"{opts} q{qi} len {len(q)}")
             sc, idx = oracle.topk(want, 10)
             assert hits[qi] == list(zip(sc.tolist(), idx.tolist()))
+
+
+@pytest.mark.parametrize("pair_shape,pair_rows", [((16, 64), 2048), ((16, 32), 2048),
+                                                  ((32, 32), 1024), ((8, 64), 512),
+                                                  ((16, 48), 1500)])
+def test_paired_queries_every_shape(ctx, pair_shape, pair_rows):
+    """Queries paired two per register (one per 16-bit lane, a pre-packed
+    profile): every paired shape, lanes spanning several passes, an odd lane
+    count, queries longer than the pair limit mixed in, and records that
+    overflow the 16-bit lanes."""
+    rng = np.random.default_rng(47)
+    lens = list(rng.integers(1, 400, size=23)) + [pair_rows, pair_rows + 1, 2600, 777]
+    qs = [synth.residues(rng, int(L)) for L in lens]
+    db = synth.small_db(15, 2000)
+    db, _ = synth.plant_homologs(rng, db, qs[-1], 0.01)
+    ctx.load_db(db.residues, db.offsets)
+    ctx.set_batch_options(pair_rows=pair_rows, pair_shape=pair_shape)
+    try:
+        for rep in range(2):                           # capture, then replay
+            hits, scores = ctx.search_batch(qs, want_scores=True)
+            for qi, q in enumerate(qs):
+                want = oracle.search(q, db.residues, db.offsets, M, 12, 2)
+                np.testing.assert_array_equal(scores[qi], want,
+                                              err_msg=f"{pair_shape} q{qi} len {len(q)}")
+                sc, idx = oracle.topk(want, 10)
+                assert hits[qi] == list(zip(sc.tolist(), idx.tolist()))
+    finally:
+        ctx.set_batch_options()
+
+
+def test_paired_queries_saturate():
+    """Paired lanes whose scores leave the 16-bit window (a matrix scoring
+    W-W at 127, runs of W): the flagged (query, record) entries go through
+    the 32-bit re-score and come out exact."""
+    m = param.blosum62().copy()
+    w = param.ALPHABET.index("W")
+    m[w, w] = 127
+    rng = np.random.default_rng(49)
+    lens = [100, 257, 258, 300, 600]
+    recs = [np.full(L, w, dtype=np.uint8) for L in lens] + \
+           [synth.residues(rng, int(L)) for L in rng.integers(5, 500, size=60)]
+    off = np.zeros(len(recs) + 1, dtype=np.uint64)
+    off[1:] = np.cumsum([len(r) for r in recs])
+    res = np.concatenate(recs)
+    qs = [np.full(L, w, dtype=np.uint8) for L in (256, 258, 400)] + \
+         [synth.residues(rng, 300), np.full(1000, w, dtype=np.uint8)]
+    with capi.Context(0, capi.default_params(top_k=5, matrix=m, reference_cap=False)) as c:
+        c.load_db(res, off)
+        hits, scores = c.search_batch(qs, want_scores=True)
+        for qi, q in enumerate(qs):
+            want = oracle.search(q, res, off, m, 12, 2, mode=0)
+            np.testing.assert_array_equal(scores[qi], want, err_msg=f"q{qi}")
+        assert c.run_stats().rescored > 0
+        assert scores[4].max() == 127 * 600
