@@ -290,6 +290,8 @@ typedef struct sw_batch_options {
                                register (pair_group_width x pair_rows_per_thread); 0 = off */
     int32_t pair_group_width;
     int32_t pair_rows_per_thread;
+    int32_t pair_long;      /* != 0: longer queries are paired too (a lane each, scored in
+                               segments of pair_rows rows by consecutive launches) */
 } sw_batch_options;
 
 /* NULL restores the defaults (no cut-over, long shape 32x16, graphs on,

@@ -68,7 +68,8 @@ class sw_batch_options(ctypes.Structure):
                 ("long_rows_per_thread", ctypes.c_int32), ("use_graph", ctypes.c_int32),
                 ("group_width", ctypes.c_int32), ("rows_per_thread", ctypes.c_int32),
                 ("stack_rows", ctypes.c_int32), ("pair_rows", ctypes.c_int32),
-                ("pair_group_width", ctypes.c_int32), ("pair_rows_per_thread", ctypes.c_int32)]
+                ("pair_group_width", ctypes.c_int32), ("pair_rows_per_thread", ctypes.c_int32),
+                ("pair_long", ctypes.c_int32)]
 
 
 class sw_image_info(ctypes.Structure):
@@ -91,7 +92,8 @@ class sw_serve_options(ctypes.Structure):
                 ("max_pending", ctypes.c_uint32), ("memory_budget", ctypes.c_uint64),
                 ("group_width", ctypes.c_int32), ("rows_per_thread", ctypes.c_int32),
                 ("stack_rows", ctypes.c_int32), ("pair_rows", ctypes.c_int32),
-                ("pair_group_width", ctypes.c_int32), ("pair_rows_per_thread", ctypes.c_int32)]
+                ("pair_group_width", ctypes.c_int32), ("pair_rows_per_thread", ctypes.c_int32),
+                ("pair_long", ctypes.c_int32)]
 
 
 class sw_serve_result(ctypes.Structure):
@@ -421,10 +423,10 @@ class Context:
 
     def set_batch_options(self, cutover=0, long_shape=(32, 16), use_graph=True,
                           stack_shape=(16, 64), stack_rows=4096, pair_rows=2048,
-                          pair_shape=(16, 64)):
+                          pair_shape=(16, 64), pair_long=True):
         o = sw_batch_options(cutover, long_shape[0], long_shape[1], 1 if use_graph else 0,
                              stack_shape[0], stack_shape[1], stack_rows, pair_rows,
-                             pair_shape[0], pair_shape[1])
+                             pair_shape[0], pair_shape[1], 1 if pair_long else 0)
         self._check(self.L.sw_set_batch_options(self.h, ctypes.byref(o)), "sw_set_batch_options")
 
     def search_batch(self, queries, want_scores: bool = False):

@@ -55,7 +55,7 @@ struct StackPlan {
     std::vector<int32_t> rb_map;
     // double stacks of the paired-query kernel: per double stack the two lanes'
     // codes offset and rows, and per (pass, thread) the (low, high) block map
-    std::vector<uint32_t> qp_off_lo, qp_rows_lo, qp_off_hi, qp_rows_hi, qp_rb_off;
+    std::vector<uint32_t> qp_off_lo, qp_rows_lo, qp_off_hi, qp_rows_hi, qp_rb_off, qp_flags;
     std::vector<int32_t> qp_rb_map;       // pairs of entries
 };
 
@@ -74,7 +74,7 @@ struct BatchGraph {
 };
 
 struct sw_batch_state {
-    sw_batch_options opt{0, 32, 16, 1, 16, 64, 4096, 2048, 16, 64};
+    sw_batch_options opt{0, 32, 16, 1, 16, 64, 4096, 2048, 16, 64, 1};
     // device
     uint8_t* d_queries = nullptr;
     size_t queries_cap = 0;
@@ -153,7 +153,7 @@ double wall_ms() {
 //   qp_rb_map[...] (16-byte aligned)            int2
 struct MetaLayout {
     size_t qoff, qlen, soff, srows, rboff, rbmap, qp_off_lo, qp_rows_lo, qp_off_hi, qp_rows_hi,
-        qp_rboff, qp_rbmap, codes, total;
+        qp_rboff, qp_flags, qp_rbmap, codes, total;
     int nst, nqp;
 };
 
@@ -173,7 +173,8 @@ MetaLayout meta_layout(uint32_t nq, const StackPlan& sp) {
     m.qp_off_hi = m.qp_rows_lo + 4 * nqp;
     m.qp_rows_hi = m.qp_off_hi + 4 * nqp;
     m.qp_rboff = m.qp_rows_hi + 4 * nqp;
-    m.qp_rbmap = (m.qp_rboff + 4 * nqp + 15) / 16 * 16;
+    m.qp_flags = m.qp_rboff + 4 * nqp;
+    m.qp_rbmap = (m.qp_flags + 4 * nqp + 15) / 16 * 16;
     m.codes = m.qp_rbmap + 4 * sp.qp_rb_map.size();
     m.total = (m.codes + sp.codes.size() + 15) / 16 * 16;
     return m;
@@ -236,6 +237,8 @@ sw_status enqueue_batch(sw_ctx* ctx, sw_batch_state* b, uint32_t nq, size_t qbyt
             q.ovf_thresh = ovf_thresh;
             q.ovf_cap = (int)std::min<size_t>(b->ovf_cap, (size_t)INT32_MAX);
             q.pair_ids = nullptr;
+            q.seg_flags = reinterpret_cast<const uint32_t*>(b->d_meta + ml.qp_flags) + L.sbegin;
+            q.seg_bnd = ctx->d_bnd;
             void* args[] = {&q};
             SW_CUDA(ctx, cudaLaunchKernel(L.qk->fn, dim3((unsigned)L.grid), dim3(L.threads), args,
                                           L.smem, st));
@@ -364,7 +367,7 @@ extern "C" sw_status sw_set_batch_options(sw_ctx* ctx, const sw_batch_options* o
             SW_SET(ctx, SW_ERR_INVALID, "bad batch options");
         ctx->batch->opt = *opt;
     } else {
-        ctx->batch->opt = sw_batch_options{0, 32, 16, 1, 16, 64, 4096, 2048, 16, 64};
+        ctx->batch->opt = sw_batch_options{0, 32, 16, 1, 16, 64, 4096, 2048, 16, 64, 1};
     }
     for (auto& kv : ctx->batch->graphs) {
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
@@ -431,8 +434,14 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
     std::vector<Bucket> buckets;
     const int sT = b->opt.group_width, sR = b->opt.rows_per_thread;
     const uint32_t cap_rows = (uint32_t)std::max(b->opt.stack_rows, 0);
+    // paired queries (sw_qpbatch, below): with pair_long every query, else the
+    // queries of at most pair_rows residues
+    const QpKernel* qk = b->opt.pair_rows > 0
+                             ? find_qp(b->opt.pair_group_width, b->opt.pair_rows_per_thread)
+                             : nullptr;
+    const bool pair_all = qk && b->opt.pair_long;
     uint32_t i0 = 0;
-    while (i0 < nz && qlen[order[i0]] >= cap_rows) {
+    while (!pair_all && i0 < nz && qlen[order[i0]] >= cap_rows) {
         const sw_kernel_config c = choose_config(ctx, (int)qlen[order[i0]]);
         if (buckets.empty() || buckets.back().T != c.short_group_width ||
             buckets.back().R != c.short_rows_per_thread || buckets.back().stacks.size() >= 1024)
@@ -443,12 +452,10 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
         buckets.back().stacks.push_back(st1);
         ++i0;
     }
-    // queries of at most pair_rows residues: paired-query double stacks (below)
-    const QpKernel* qk = b->opt.pair_rows > 0
-                             ? find_qp(b->opt.pair_group_width, b->opt.pair_rows_per_thread)
-                             : nullptr;
     uint32_t ip = nz;
-    if (qk)
+    if (pair_all)
+        ip = 0;
+    else if (qk)
         while (ip > i0 && qlen[order[ip - 1]] <= (uint32_t)b->opt.pair_rows) --ip;
     if (i0 < ip) {
         Bucket bk{sT, sR, {}};
@@ -547,12 +554,15 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
             launches.push_back(L);
         }
     }
-    // paired queries: lanes of at most pair_rows rows (first fit, longest
-    // first, each query padded to whole R-row blocks), consecutive lanes
-    // paired into double stacks, all in one launch
+    // paired queries: lanes of at most `seg` rows (first fit, longest first,
+    // each query padded to whole R-row blocks; a longer query gets a lane of
+    // its own), consecutive lanes paired into double stacks.  A double stack
+    // taller than `seg` rows is cut into segments of `seg` rows, scored by
+    // consecutive launches; segment s takes its upper boundary row from
+    // segment s-1 through the per-record boundary buffer.
     if (qk && ip < nz) {
-        const uint32_t qR = (uint32_t)qk->R, qT = (uint32_t)qk->T;
-        const uint32_t lane_cap = std::max<uint32_t>((uint32_t)b->opt.pair_rows, qR);
+        const uint32_t qR = (uint32_t)qk->R, qT = (uint32_t)qk->T, pass_rows = qT * qR;
+        const uint32_t seg = std::max(pass_rows, (uint32_t)b->opt.pair_rows / pass_rows * pass_rows);
         struct Lane {
             std::vector<uint32_t> q;
             uint32_t rows = 0;
@@ -562,24 +572,28 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
             const uint32_t q = order[i];
             const uint32_t need = (qlen[q] + qR - 1) / qR * qR;
             bool placed = false;
-            for (Lane& ln : lanes)
-                if (ln.rows + need <= lane_cap) {
-                    ln.q.push_back(q);
-                    ln.rows += need;
-                    placed = true;
-                    break;
-                }
+            if (need <= seg)
+                for (Lane& ln : lanes)
+                    if (ln.rows + need <= seg) {
+                        ln.q.push_back(q);
+                        ln.rows += need;
+                        placed = true;
+                        break;
+                    }
             if (!placed) lanes.push_back(Lane{{q}, need});
         }
         if (lanes.size() % 2) lanes.push_back(Lane{});      // an empty high lane
-        uint32_t max_rows = 0;
-        for (size_t d = 0; d < lanes.size(); d += 2) {
-            const Lane* pair_l[2] = {&lanes[d], &lanes[d + 1]};
+        struct Double {
+            uint32_t off[2], rows[2], nseg;
             std::vector<int32_t> blocks[2];
+        };
+        std::vector<Double> dbl(lanes.size() / 2);
+        for (size_t d = 0; d < dbl.size(); ++d) {
+            Double& D = dbl[d];
             for (int h = 0; h < 2; ++h) {
-                const Lane& ln = *pair_l[h];
-                (h ? sp.qp_off_hi : sp.qp_off_lo).push_back((uint32_t)sp.codes.size());
-                (h ? sp.qp_rows_hi : sp.qp_rows_lo).push_back(ln.rows);
+                const Lane& ln = lanes[2 * d + h];
+                D.off[h] = (uint32_t)sp.codes.size();
+                D.rows[h] = ln.rows;
                 for (const uint32_t q : ln.q) {
                     const uint8_t* src = queries + qoffsets[q];
                     const uint32_t L = qlen[q];
@@ -587,43 +601,70 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
                     sp.codes.insert(sp.codes.end(), src, src + L);
                     sp.codes.insert(sp.codes.end(), padded - L, (uint8_t)kZeroCode);
                     for (uint32_t j = 0; j < padded / qR; ++j)
-                        blocks[h].push_back((int32_t)q | (j == 0 ? kFirstBit : 0));
+                        D.blocks[h].push_back((int32_t)q | (j == 0 ? kFirstBit : 0));
                 }
             }
-            const uint32_t rows = std::max(lanes[d].rows, lanes[d + 1].rows);
-            max_rows = std::max(max_rows, rows);
-            const uint32_t P = (rows + qT * qR - 1) / (qT * qR);
-            sp.qp_rb_off.push_back((uint32_t)(sp.qp_rb_map.size() / 2));
-            for (uint32_t j = 0; j < P * qT; ++j) {
-                sp.qp_rb_map.push_back(j < blocks[0].size() ? blocks[0][j] : -1);
-                sp.qp_rb_map.push_back(j < blocks[1].size() ? blocks[1][j] : -1);
+            D.nseg = std::max<uint32_t>(1, (std::max(D.rows[0], D.rows[1]) + seg - 1) / seg);
+        }
+        // launches: every single-segment double stack in one launch; then each
+        // taller double stack's segments in launches of their own, one after
+        // another (they share the per-record boundary buffer)
+        std::vector<std::vector<std::pair<size_t, uint32_t>>> groups(1);   // (double stack, segment)
+        for (size_t d = 0; d < dbl.size(); ++d)
+            if (dbl[d].nseg == 1) groups[0].push_back({d, 0u});
+        for (size_t d = 0; d < dbl.size(); ++d)
+            for (uint32_t lv = 0; dbl[d].nseg > 1 && lv < dbl[d].nseg; ++lv)
+                groups.push_back({{d, lv}});
+        for (const auto& grp : groups) {
+            if (grp.empty()) continue;
+            const int first = (int)sp.qp_off_lo.size();
+            uint32_t max_rows = 0;
+            for (const auto& e : grp) {
+                const Double& D = dbl[e.first];
+                const uint32_t lv = e.second;
+                uint32_t rs[2];
+                for (int h = 0; h < 2; ++h) {
+                    rs[h] = D.rows[h] > lv * seg ? std::min(seg, D.rows[h] - lv * seg) : 0u;
+                    (h ? sp.qp_off_hi : sp.qp_off_lo).push_back(D.off[h] + lv * seg);
+                    (h ? sp.qp_rows_hi : sp.qp_rows_lo).push_back(rs[h]);
+                }
+                const uint32_t rows = std::max(rs[0], rs[1]);
+                max_rows = std::max(max_rows, rows);
+                const uint32_t P = std::max<uint32_t>(1, (rows + pass_rows - 1) / pass_rows);
+                sp.qp_rb_off.push_back((uint32_t)(sp.qp_rb_map.size() / 2));
+                sp.qp_flags.push_back((lv > 0 ? 1u : 0u) | (lv + 1 < D.nseg ? 2u : 0u));
+                const size_t b0 = (size_t)lv * seg / qR;
+                for (uint32_t j = 0; j < P * qT; ++j)
+                    for (int h = 0; h < 2; ++h)
+                        sp.qp_rb_map.push_back(b0 + j < D.blocks[h].size() ? D.blocks[h][b0 + j] : -1);
             }
+            const size_t smem = qk->smem((int)std::max<uint32_t>(max_rows, 1));
+            int occ = 0;
+            if (smem <= (size_t)ctx->max_smem &&
+                cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, qk->fn, qk->block, smem) !=
+                    cudaSuccess) {
+                cudaGetLastError();
+                occ = 0;
+            }
+            if (occ == 0)
+                SW_SET(ctx, SW_ERR_UNSUPPORTED, "paired segments of %u rows do not fit shape %dx%d",
+                       max_rows, qk->T, qk->R);
+            BatchLaunch L;
+            L.qk = qk;
+            L.k = nullptr;
+            L.threads = qk->block;
+            L.grid = occ * ctx->num_sms;
+            L.smem = smem;
+            L.sbegin = first;
+            L.scount = (int)sp.qp_off_lo.size() - first;
+            L.pair_begin = 0;
+            L.pair_count = (int)ctx->n_pairs;
+            L.counter_base = 2 * nst_total + 1 + first;
+            L.long_part = false;
+            L.bnd_group = 2 * (size_t)ctx->max_cols;
+            bnd_bulk = std::max(bnd_bulk, (size_t)L.grid * (L.threads / qk->T) * L.bnd_group);
+            launches.push_back(L);
         }
-        const size_t smem = qk->smem((int)max_rows);
-        int occ = 0;
-        if (smem <= (size_t)ctx->max_smem &&
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, qk->fn, qk->block, smem) != cudaSuccess) {
-            cudaGetLastError();
-            occ = 0;
-        }
-        if (occ == 0)
-            SW_SET(ctx, SW_ERR_UNSUPPORTED, "paired lanes of %u rows do not fit shape %dx%d",
-                   max_rows, qk->T, qk->R);
-        BatchLaunch L;
-        L.qk = qk;
-        L.k = nullptr;
-        L.threads = qk->block;
-        L.grid = occ * ctx->num_sms;
-        L.smem = smem;
-        L.sbegin = 0;
-        L.scount = (int)sp.qp_off_lo.size();
-        L.pair_begin = 0;
-        L.pair_count = (int)ctx->n_pairs;
-        L.counter_base = 2 * nst_total + 1;
-        L.long_part = false;
-        L.bnd_group = 2 * (size_t)ctx->max_cols;
-        bnd_bulk = std::max(bnd_bulk, (size_t)L.grid * (L.threads / qk->T) * L.bnd_group);
-        launches.push_back(L);
     }
     // counters: bulk of stack i at [i], long at [nst_total + i], overflow count
     // at [2 nst_total], paired double stack j at [2 nst_total + 1 + j]
@@ -721,6 +762,7 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
         memcpy(m + ml.qp_off_hi, sp.qp_off_hi.data(), 4 * nqp);
         memcpy(m + ml.qp_rows_hi, sp.qp_rows_hi.data(), 4 * nqp);
         memcpy(m + ml.qp_rboff, sp.qp_rb_off.data(), 4 * nqp);
+        memcpy(m + ml.qp_flags, sp.qp_flags.data(), 4 * nqp);
         memcpy(m + ml.qp_rbmap, sp.qp_rb_map.data(), 4 * sp.qp_rb_map.size());
         memcpy(m + ml.codes, sp.codes.data(), sp.codes.size());
     }
@@ -734,7 +776,8 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
     sig.push_back((uint64_t)b->opt.group_width << 32 | (uint32_t)b->opt.rows_per_thread);
     sig.push_back((uint64_t)b->opt.stack_rows);
     sig.push_back((uint64_t)b->opt.pair_rows << 32 |
-                  (uint64_t)(b->opt.pair_group_width * 256 + b->opt.pair_rows_per_thread));
+                  (uint64_t)(b->opt.pair_group_width * 256 + b->opt.pair_rows_per_thread) << 1 |
+                  (uint64_t)(b->opt.pair_long != 0));
     for (uint32_t i = 0; i < nq; ++i) sig.push_back(qlen[i]);
     uint32_t n_launch = 0;
     SW_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));

@@ -52,6 +52,12 @@ struct QpArgs {
     int ovf_thresh;
     int ovf_cap;
     const uint32_t* pair_ids;   // optional: global pair of each entry of pairs
+    // segments: a double stack taller than one launch's limit is cut into row
+    // segments scored by consecutive launches; per stack, bit 0 = read the
+    // rows above from seg_bnd at pass 0, bit 1 = write the last row to it
+    const uint32_t* seg_flags;
+    uint2* seg_bnd;             // per record and column: (H, F) of a segment's last row,
+                                // at 16 entries per 16-byte stream unit (2 per column)
 };
 
 // Shared-memory bytes of a double stack's profile (rows = the taller lane).
@@ -125,7 +131,7 @@ __device__ __forceinline__ void reverse_sweep_qp(uint32_t (&H)[R], const uint32_
 // against both lanes' stacks.  Returns when the units are exhausted.
 template <int T, int R>
 __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, int P, int* counter,
-                                           const int2* rb_map) {
+                                           const int2* rb_map, uint32_t seg) {
     static_assert(R % 8 == 0, "R");
     constexpr int NJ = R / 4;
     constexpr int HALF = R / 2;
@@ -157,6 +163,8 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
     Pair2 ninfo{0u, 0u};
     int q_lo = -1, q_hi = -1;
     uint32_t reset = 0u;     // lanes whose query starts at this thread's first row
+    bool has_in = false;     // the pass takes its rows above from a boundary row
+    const uint2* in_b = pbnd;
 
 #define SWQ_START_PASS()                                                   \
     {                                                                      \
@@ -179,13 +187,15 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
         mid_f = Z;                                                         \
         d_bot = kZeroCode;                                                 \
         d_out = kZeroCode;                                                 \
+        has_in = pass > 0 || (seg & 1u);                                   \
+        in_b = pass > 0 ? pbnd + ((pass - 1) & 1)                          \
+                        : a.seg_bnd + (size_t)off16 * 16 + half;           \
         if (t == 0) {                                                      \
             dcur = __ldg(a.db + off16);                                    \
             if (ncols > 8) dnext = __ldg(a.db + off16 + 1);                \
-            if (pass > 0) {                                                \
-                const uint2* pb = pbnd + ((pass - 1) & 1);                 \
-                bq0 = pb[0];                                               \
-                if (ncols > 1) bq1 = pb[2];                                \
+            if (has_in) {                                                  \
+                bq0 = in_b[0];                                             \
+                if (ncols > 1) bq1 = in_b[2];                              \
             }                                                              \
         }                                                                  \
     }
@@ -234,11 +244,11 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
                 dcur.y = __funnelshift_r(dcur.y, dcur.z, 16);
                 dcur.z = __funnelshift_r(dcur.z, dcur.w, 16);
                 dcur.w >>= 16;
-                if (pass > 0) {
+                if (has_in) {
                     h_in = bq0.x;
                     f_in = bq0.y;
                     bq0 = bq1;
-                    if (s + 2 < ncols) bq1 = pbnd[2 * (s + 2) + ((pass - 1) & 1)];
+                    if (s + 2 < ncols) bq1 = in_b[2 * (s + 2)];
                 }
                 // the next unit's pair entry, once its claim has returned
                 if (pass == 0 && s == (ncols < 9 ? ncols - 1 : 8) && next < units)
@@ -274,8 +284,13 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
             if (bot_valid) {
                 out_h = H[R - 1];
                 out_f = f_bot;
-                if (t == T - 1 && pass + 1 < P)
-                    pbnd[2 * (ct - 1) + (pass & 1)] = make_uint2(out_h, out_f);
+                if (t == T - 1) {
+                    if (pass + 1 < P)
+                        pbnd[2 * (ct - 1) + (pass & 1)] = make_uint2(out_h, out_f);
+                    else if (seg & 2u)
+                        a.seg_bnd[(size_t)off16 * 16 + 2 * (ct - 1) + half] =
+                            make_uint2(out_h, out_f);
+                }
             }
         }
         prev_h = h_in;
@@ -344,7 +359,8 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_qpbatch(const QpArgs a) {
         build_profile_qp<T, R>(prof4, a.codes + a.off_lo[i], (int)a.rows_lo[i],
                                a.codes + a.off_hi[i], (int)a.rows_hi[i], a.mat, P);
         __syncthreads();
-        run_qpairs<T, R>(a, prof4, P, a.counters + i, a.rb_map + a.rb_off[i]);
+        run_qpairs<T, R>(a, prof4, P, a.counters + i, a.rb_map + a.rb_off[i],
+                         a.seg_flags ? a.seg_flags[i] : 0u);
     }
 }
 

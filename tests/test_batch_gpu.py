@@ -104,21 +104,23 @@ def test_many_short_queries_share_stacks(ctx):
             assert hits[qi] == list(zip(sc.tolist(), idx.tolist()))
 
 
-@pytest.mark.parametrize("pair_shape,pair_rows", [((16, 64), 2048), ((16, 32), 2048),
-                                                  ((32, 32), 1024), ((8, 64), 512),
-                                                  ((16, 48), 1500)])
-def test_paired_queries_every_shape(ctx, pair_shape, pair_rows):
+@pytest.mark.parametrize("pair_shape,pair_rows,pair_long", [
+    ((16, 64), 2048, True), ((16, 64), 2048, False), ((16, 32), 2048, True),
+    ((32, 32), 1024, True), ((8, 64), 512, True), ((16, 48), 1500, False),
+    ((16, 64), 1024, True)])
+def test_paired_queries_every_shape(ctx, pair_shape, pair_rows, pair_long):
     """Queries paired two per register (one per 16-bit lane, a pre-packed
     profile): every paired shape, lanes spanning several passes, an odd lane
-    count, queries longer than the pair limit mixed in, and records that
-    overflow the 16-bit lanes."""
+    count, and queries longer than the pair limit -- paired too, in segments
+    scored by consecutive launches (pair_long), or left to the stacked
+    kernel."""
     rng = np.random.default_rng(47)
-    lens = list(rng.integers(1, 400, size=23)) + [pair_rows, pair_rows + 1, 2600, 777]
+    lens = list(rng.integers(1, 400, size=23)) + [pair_rows, pair_rows + 1, 2600, 777, 5000, 4097]
     qs = [synth.residues(rng, int(L)) for L in lens]
     db = synth.small_db(15, 2000)
     db, _ = synth.plant_homologs(rng, db, qs[-1], 0.01)
     ctx.load_db(db.residues, db.offsets)
-    ctx.set_batch_options(pair_rows=pair_rows, pair_shape=pair_shape)
+    ctx.set_batch_options(pair_rows=pair_rows, pair_shape=pair_shape, pair_long=pair_long)
     try:
         for rep in range(2):                           # capture, then replay
             hits, scores = ctx.search_batch(qs, want_scores=True)
