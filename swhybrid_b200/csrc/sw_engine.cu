@@ -671,6 +671,18 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
             ctx->stats.used.long_rows_per_thread = lk->R;
         }
     }
+    // every shape is checked before anything is launched: a search refused
+    // half-way would leave a launch in flight that writes into the next one
+    for (int si = split ? 1 : 0; si < 2; ++si) {
+        const Seg& sg = segs[si];
+        if (sg.e <= sg.b) continue;
+        const WfKernel* k = find_kernel(sg.T, sg.R);
+        if (!k) SW_SET(ctx, SW_ERR_INVALID, "no kernel %dx%d", sg.T, sg.R);
+        if (shape_occupancy(ctx, *k, qlen) == 0)
+            SW_SET(ctx, SW_ERR_UNSUPPORTED,
+                   "query of %d residues does not fit shape %dx%d (profile %zu bytes)", qlen,
+                   sg.T, sg.R, k->smem(qlen));
+    }
     int reserved_sms = 0;
     if (split) {
         uint64_t long_cols = 0;

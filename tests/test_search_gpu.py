@@ -185,6 +185,22 @@ def test_automatic_cutover_on_a_long_tailed_db(ctx, long_case):
         ctx.set_kernel_config(None)
 
 
+def test_refused_search_leaves_nothing_in_flight(ctx, long_case):
+    """A search refused because its query does not fit the shape (with a
+    long-pair split configured) launches nothing, so the next search is exact."""
+    db, lq, lwant = long_case
+    ctx.load_db(db.residues, db.offsets)
+    try:
+        ctx.set_kernel_config((32, 16, 4, 32, 1500))
+        with pytest.raises(capi.SwError) as e:
+            ctx.search(lq[3])                      # 4,097 rows: too big for 4x32
+        assert e.value.status == 6
+        _, scores = ctx.search(lq[0], want_scores=True)
+        np.testing.assert_array_equal(scores, lwant[0])
+    finally:
+        ctx.set_kernel_config(None)
+
+
 def test_other_gap_costs_match_oracle():
     rng = np.random.default_rng(22)
     db = synth.small_db(5, 800)
