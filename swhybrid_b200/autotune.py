@@ -117,7 +117,7 @@ def main():
     ap.add_argument("--records", type=int, default=570_000)
     ap.add_argument("--long", type=int, default=200)
     ap.add_argument("--reps", type=int, default=1)
-    ap.add_argument("--widths", type=str, default="8,16,32",
+    ap.add_argument("--widths", type=str, default="4,8,16,32",
                     help="group widths to try (comma separated)")
     args = ap.parse_args()
     widths = [int(x) for x in args.widths.split(",")]
