@@ -189,6 +189,25 @@ sw_status sw_fasta_to_image(const char *fasta_path, const char *image_path,
  * reports its sizes.  Needs no device. */
 sw_status sw_image_get_info(const char *path, int verify_checksum, sw_image_info *info);
 
+/* Read access to an image without a device: maps the file (checked as by
+ * sw_image_get_info) and points into it.  The pointers stay valid until
+ * sw_image_close.  For host code that needs the records or titles
+ * themselves, such as a DataPool reading a DB for several workers. */
+typedef struct sw_image_view {
+    const uint8_t *residues;        /* codes 0..24, records back to back */
+    const uint64_t *offsets;        /* n_records + 1 */
+    const char *titles;
+    const uint64_t *title_offsets;  /* n_records + 1 */
+    const uint32_t *order;          /* records by length, longest first, stable */
+    uint64_t n_records;
+    uint64_t n_residues;
+    const void *mapping;            /* for sw_image_close */
+    uint64_t mapping_bytes;
+} sw_image_view;
+
+sw_status sw_image_open(const char *path, int verify_checksum, sw_image_view *view);
+void sw_image_close(sw_image_view *view);
+
 /* sw_db_load from an image: maps the file, checks it as sw_image_get_info
  * does, builds the device layout from the stored order (checked to be the
  * stable longest-first permutation) and keeps the file mapped for titles. */

@@ -33,6 +33,7 @@ EXPORTS = [
     "sw_serve_poll", "sw_serve_get_stats", "sw_serve_clock_ms", "sw_serve_stop",
     "sw_traceback", "sw_db_write_image", "sw_fasta_to_image", "sw_image_get_info",
     "sw_db_load_image", "sw_db_title", "sw_params_parse_matrix", "sw_params_load_matrix",
+    "sw_image_open", "sw_image_close",
 ]
 
 

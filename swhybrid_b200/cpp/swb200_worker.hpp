@@ -144,6 +144,33 @@ public:
         d.query.assign(q.begin() + qo[0], q.begin() + qo[1]);
         return d;
     }
+    // The records and titles of a DB image (sw_fasta_to_image), the query from FASTA.
+    static DataPool from_image(const std::string& imagePath, const std::string& queryPath) {
+        DataPool d;
+        sw_image_view v;
+        if (sw_image_open(imagePath.c_str(), 1, &v) != SW_OK)
+            throw std::runtime_error(std::string("DB image: ") + sw_last_error(nullptr));
+        d.residues.assign(v.residues, v.residues + v.n_residues);
+        d.offsets.assign(v.offsets, v.offsets + v.n_records + 1);
+        d.titles.reserve(v.n_records);
+        for (uint64_t i = 0; i < v.n_records; ++i)
+            d.titles.emplace_back(v.titles + v.title_offsets[i],
+                                  v.title_offsets[i + 1] - v.title_offsets[i]);
+        sw_image_close(&v);
+        std::vector<std::string> qt;
+        std::vector<uint8_t> q;
+        std::vector<uint64_t> qo;
+        d.read_fasta(queryPath, &qt, &q, &qo);
+        if (qo.size() < 2) throw std::runtime_error("no query record in " + queryPath);
+        d.query.assign(q.begin() + qo[0], q.begin() + qo[1]);
+        return d;
+    }
+    // An image when the file is one, else FASTA.
+    static DataPool open(const std::string& dbPath, const std::string& queryPath) {
+        sw_image_info info;
+        if (sw_image_get_info(dbPath.c_str(), 0, &info) == SW_OK) return from_image(dbPath, queryPath);
+        return from_fasta(dbPath, queryPath);
+    }
     const uint8_t* getQuery() const { return query.data(); }
     size_t getQueryLen() const { return query.size(); }
     size_t getTotalResidue() const { return residues.size(); }

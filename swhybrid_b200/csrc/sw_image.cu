@@ -381,6 +381,31 @@ extern "C" sw_status sw_image_get_info(const char* path, int verify_checksum,
     return SW_OK;
 }
 
+extern "C" sw_status sw_image_open(const char* path, int verify_checksum, sw_image_view* view) {
+    if (!view) return thread_fail(SW_ERR_INVALID, "null argument");
+    memset(view, 0, sizeof(*view));
+    Mapped m;
+    sw_status st = map_image(path, verify_checksum != 0, &m);
+    if (st != SW_OK) return st;
+    const ImageHeader& h = *m.h;
+    view->residues = m.base + h.off_residues;
+    view->offsets = (const uint64_t*)(m.base + h.off_offsets);
+    view->titles = (const char*)(m.base + h.off_titles);
+    view->title_offsets = (const uint64_t*)(m.base + h.off_title_offsets);
+    view->order = (const uint32_t*)(m.base + h.off_order);
+    view->n_records = h.n_records;
+    view->n_residues = h.n_residues;
+    view->mapping = m.base;
+    view->mapping_bytes = m.bytes;
+    return SW_OK;
+}
+
+extern "C" void sw_image_close(sw_image_view* view) {
+    if (!view || !view->mapping) return;
+    munmap((void*)view->mapping, view->mapping_bytes);
+    memset(view, 0, sizeof(*view));
+}
+
 extern "C" sw_status sw_db_load_image(sw_ctx* ctx, const char* path, int verify_checksum) {
     if (!ctx) return SW_ERR_INVALID;
     if (ctx->serve) return SW_ERR_BUSY;   // the serving loop owns the stream and the DB

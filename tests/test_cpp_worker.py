@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import oracle
-from swhybrid_b200 import param, synth
+from swhybrid_b200 import capi, param, synth
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 RL = os.path.join(ROOT, "swhybrid_b200", "cpp", "result_list_test")
@@ -67,3 +67,26 @@ def test_worker_pool_end_to_end(tmp_path):
     sc, idx = oracle.topk(want, 10)
     assert hits == list(zip(sc.tolist(), idx.tolist()))
     assert f"score {sc[0]} -- >rec{idx[0]} synthetic" in out.stdout
+
+
+@pytest.mark.gpu
+def test_worker_pool_from_db_image(tmp_path):
+    """The same pool fed from a DB image made by the FASTA converter: same
+    hits, titles from the image's title index (the header without '>')."""
+    rng = np.random.default_rng(18)
+    db = synth.small_db(22, 1200)
+    q = synth.residues(rng, 300)
+    db, _ = synth.plant_homologs(rng, db, q, 0.01)
+    dbf, qf, img = tmp_path / "db.fa", tmp_path / "q.fa", tmp_path / "db.swdb"
+    write_fasta(dbf, [db.record(i) for i in range(db.n)], "rec")
+    write_fasta(qf, [q], "query")
+    capi.fasta_to_image(str(dbf), str(img))
+    out = subprocess.run([WP, "-q", str(qf), "-db", str(img), "-t", "10", "-g", "1"],
+                         capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    hits = [tuple(map(int, ln.split()[1:3])) for ln in out.stdout.splitlines()
+            if ln.startswith("HIT ")]
+    want = oracle.search(q, db.residues, db.offsets, param.blosum62(), 12, 2)
+    sc, idx = oracle.topk(want, 10)
+    assert hits == list(zip(sc.tolist(), idx.tolist()))
+    assert f"score {sc[0]} -- rec{idx[0]} synthetic" in out.stdout
