@@ -292,8 +292,9 @@ def serve_leg(ctx, db, n_req: int, seed: int = 5):
         levels = []
         check_ids = []
         base = 1_000_000
+        level_qs = requests(n_req)           # the same requests at every offered load
         for frac in (0.25, 0.5, 0.75, 1.0):
-            qs = requests(n_req)
+            qs = level_qs
             arr = _synth.poisson_arrivals(rng, n_req, frac * sat_rate)
             st0 = ctx.serve_stats()
             t_start = time.perf_counter()
@@ -333,7 +334,7 @@ def serve_leg(ctx, db, n_req: int, seed: int = 5):
     return {
         "workload": "requests of lengths log-uniform 30..8,000 (seeded) against the full-size DB; "
                     "saturating rate from %d requests queued at once, then Poisson arrivals at "
-                    "25/50/75/100%% of it, %d requests per level" % (3 * slots, n_req),
+                    "25/50/75/100%% of it, the same %d requests at every level" % (3 * slots, n_req),
         "slots": slots, "chunks": int(st.chunks),
         "saturated": {"requests": len(sat_q), "rate_per_s": round(sat_rate, 3),
                       "gcups": round(sat_cells / ((t1 - t0) * 1e-3) / 1e9, 1)},
