@@ -16,10 +16,11 @@
 // work on column c-1, so every step runs two independent F chains side by side
 // (twice the instruction-level parallelism of one R-row chain).  Thread t's
 // top half trails thread t-1's bottom half by one step (anti-diagonal
-// wavefront): through warp shuffles it receives the H/F of the row above and
-// the residue pair.  Thread 0 streams the pair's columns (prefetched 16-byte
-// chunks).  A query longer than T*R rows is done in passes; between passes
-// the last row's H/F per column goes through a double-buffered boundary row
+// wavefront): through warp shuffles it receives the H/F of the row above;
+// each thread loads its own column's residue pair one step ahead (2-byte
+// loads that the group's threads make from one 64-byte span).  A query
+// longer than T*R rows is done in passes; between passes the last row's H/F
+// per column goes through a double-buffered boundary row
 // in global memory (written by thread T-1, read back two columns ahead by
 // thread 0).  T = 1 is the inter-sequence form (one pair per thread); T > 1
 // is the warp-cooperative intra-sequence form.
@@ -229,14 +230,14 @@ __device__ __forceinline__ void run_pairs(const RunArgs& a, const uint2* prof) {
     uint32_t H[R], E[R];
     uint32_t S = Z;
     uint32_t out_h = Z, out_f = Z, prev_h = Z, mid_h = Z, mid_f = Z;
-    uint32_t d_bot = kPadPair, d_out = kPadPair;
+    uint32_t d_bot = kPadPair, d_cur = kPadPair;
+    const unsigned short* col = reinterpret_cast<const unsigned short*>(a.db);
     int pair = 0, next = 0, pass = 0, s = 0, nsteps = 0, ncols = 0;
     uint32_t off16 = 0u;
     uint2* pbnd = grp_bnd;
     bool done = false;
-    // thread 0 of a group: residue chunks (current, next), boundary entries of
-    // the next two columns, and the next pair (claimed one pair ahead)
-    uint4 dcur = make_uint4(0u, 0u, 0u, 0u), dnext = dcur;
+    // thread 0 of a group: boundary entries of the next two columns, and the
+    // next pair (claimed one pair ahead)
     uint2 bq0 = make_uint2(Z, Z), bq1 = bq0;
     Pair2 ninfo{0u, 0u};
     int my_q = 0;           // stacked: this thread's query in the current pass
@@ -262,10 +263,9 @@ __device__ __forceinline__ void run_pairs(const RunArgs& a, const uint2* prof) {
         mid_h = Z;                                                         \
         mid_f = Z;                                                         \
         d_bot = kPadPair;                                                  \
-        d_out = kPadPair;                                                  \
+        col = reinterpret_cast<const unsigned short*>(a.db) + (size_t)off16 * 8; \
+        d_cur = (t == 0 && ncols > 0) ? (uint32_t)__ldg(col) : kPadPair;  \
         if (t == 0) {                                                      \
-            dcur = __ldg(a.db + off16);                                    \
-            if (ncols > 8) dnext = __ldg(a.db + off16 + 1);                \
             if (pass > 0) {                                                \
                 const uint2* pb = pbnd + ((pass - 1) & 1);                 \
                 bq0 = pb[0];                                               \
@@ -302,25 +302,20 @@ __device__ __forceinline__ void run_pairs(const RunArgs& a, const uint2* prof) {
     }
 
     while (!__all_sync(FULL, done)) {
-        // thread t-1's bottom half handed down the column it processed in the
-        // previous step, with that column's last-row H and F
-        uint32_t d_in = __shfl_up_sync(FULL, d_out, 1, T);
+        // thread t-1's bottom half handed down the last-row H and F of the
+        // column it processed in the previous step; every thread loads its
+        // own column's residue pair one step ahead
         uint32_t h_in = __shfl_up_sync(FULL, out_h, 1, T);
         uint32_t f_in = __shfl_up_sync(FULL, out_f, 1, T);
+        const uint32_t d_in = d_cur;
+        {
+            const int c1 = s + 1 - 2 * t;     // this thread's top column next step
+            d_cur = (c1 >= 0 && c1 < ncols) ? (uint32_t)__ldg(col + c1) : kPadPair;
+        }
         if (t == 0) {
-            d_in = kPadPair;
             h_in = Z;
             f_in = Z;
             if (s < ncols) {
-                if (s > 0 && (s & 7) == 0) {
-                    dcur = dnext;
-                    if (s + 8 < ncols) dnext = __ldg(a.db + off16 + (s >> 3) + 1);
-                }
-                d_in = dcur.x & 0xffffu;
-                dcur.x = __funnelshift_r(dcur.x, dcur.y, 16);
-                dcur.y = __funnelshift_r(dcur.y, dcur.z, 16);
-                dcur.z = __funnelshift_r(dcur.z, dcur.w, 16);
-                dcur.w >>= 16;
                 if (pass > 0) {
                     h_in = bq0.x;
                     f_in = bq0.y;
@@ -371,7 +366,6 @@ __device__ __forceinline__ void run_pairs(const RunArgs& a, const uint2* prof) {
             }
         }
         prev_h = h_in;
-        d_out = d_bot;
         d_bot = d_in;
         ++s;
         if (!done && s == nsteps) {  // uniform within the group
