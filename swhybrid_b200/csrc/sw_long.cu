@@ -82,8 +82,8 @@ __global__ void __launch_bounds__(LongBlock<R>::value, 1) sw_long(const LongArgs
     const uint2* const ring_in = links + (size_t)(w > 0 ? w - 1 : 0) * kLRing;  // link w-1 -> w
     uint32_t H[R], E[R];
     uint32_t S = Z, out_h = Z, out_f = Z, prev_h = Z, mid_h = Z, mid_f = Z;
-    uint32_t d_bot = kPadPair, d_out = kPadPair;
-    uint4 dcur = make_uint4(0u, 0u, 0u, 0u), dnext = dcur;
+    uint32_t d_bot = kPadPair, d_cur = kPadPair;
+    const unsigned short* col = reinterpret_cast<const unsigned short*>(a.db);
     int pair = 0, ncols = 0, span = 0, total = 0, start = 0;
     uint32_t off16 = 0u;
     bool active = false;
@@ -111,11 +111,8 @@ __global__ void __launch_bounds__(LongBlock<R>::value, 1) sw_long(const LongArgs
             mid_h = Z;                                                     \
             mid_f = Z;                                                     \
             d_bot = kPadPair;                                              \
-            d_out = kPadPair;                                              \
-            if (t == 0) {                                                  \
-                dcur = __ldg(a.db + off16);                                \
-                if (ncols > 8) dnext = __ldg(a.db + off16 + 1);            \
-            }                                                              \
+            col = reinterpret_cast<const unsigned short*>(a.db) + (size_t)off16 * 8; \
+            d_cur = (t == 0 && ncols > 0) ? (uint32_t)__ldg(col) : kPadPair; \
         }                                                                  \
     }
     if (leader) s_next[g] = atomicAdd(a.counter, 1);
@@ -126,23 +123,17 @@ __global__ void __launch_bounds__(LongBlock<R>::value, 1) sw_long(const LongArgs
         for (int j = 0; j < kLK; ++j, ++gs) {
             const int s = gs - start - w * kLD;            // this warp's step (warp-uniform)
             if (!active || s < 0 || s >= span) continue;
-            uint32_t d_in = __shfl_up_sync(FULL, d_out, 1);
             uint32_t h_in = __shfl_up_sync(FULL, out_h, 1);
             uint32_t f_in = __shfl_up_sync(FULL, out_f, 1);
+            const uint32_t d_in = d_cur;       // this thread's top column, loaded a step ahead
+            {
+                const int c1 = s + 1 - 2 * t;
+                d_cur = (c1 >= 0 && c1 < ncols) ? (uint32_t)__ldg(col + c1) : kPadPair;
+            }
             if (t == 0) {
-                d_in = kPadPair;
                 h_in = Z;
                 f_in = Z;
                 if (s < ncols) {
-                    if (s > 0 && (s & 7) == 0) {
-                        dcur = dnext;
-                        if (s + 8 < ncols) dnext = __ldg(a.db + off16 + (s >> 3) + 1);
-                    }
-                    d_in = dcur.x & 0xffffu;
-                    dcur.x = __funnelshift_r(dcur.x, dcur.y, 16);
-                    dcur.y = __funnelshift_r(dcur.y, dcur.z, 16);
-                    dcur.z = __funnelshift_r(dcur.z, dcur.w, 16);
-                    dcur.w >>= 16;
                     if (w > 0) {
                         const uint2 b = ring_in[s & (kLRing - 1)];
                         h_in = b.x;
@@ -182,7 +173,6 @@ __global__ void __launch_bounds__(LongBlock<R>::value, 1) sw_long(const LongArgs
                 }
             }
             prev_h = h_in;
-            d_out = d_bot;
             d_bot = d_in;
         }
         // barrier: pipelines whose pair ends here publish their passes' maxima

@@ -154,11 +154,11 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
 
     uint32_t H[R], E[R];
     uint32_t S = Z, out_h = Z, out_f = Z, prev_h = Z, mid_h = Z, mid_f = Z;
-    uint32_t d_bot = kZeroCode, d_out = kZeroCode;
+    uint32_t d_bot = kZeroCode, d_cur = kZeroCode;
+    const unsigned short* col = reinterpret_cast<const unsigned short*>(a.db);
     int unit = 0, next = 0, pass = 0, s = 0, nsteps = 0, ncols = 0, half = 0;
     uint32_t off16 = 0u;
     bool done = false;
-    uint4 dcur = make_uint4(0u, 0u, 0u, 0u), dnext = dcur;
     uint2 bq0 = make_uint2(Z, Z), bq1 = bq0;
     Pair2 ninfo{0u, 0u};
     int q_lo = -1, q_hi = -1;
@@ -186,13 +186,13 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
         mid_h = Z;                                                         \
         mid_f = Z;                                                         \
         d_bot = kZeroCode;                                                 \
-        d_out = kZeroCode;                                                 \
+        col = reinterpret_cast<const unsigned short*>(a.db) + (size_t)off16 * 8; \
+        d_cur = (t == 0 && ncols > 0) ? (((uint32_t)__ldg(col) >> (8 * half)) & 0xffu) \
+                                      : (uint32_t)kZeroCode;               \
         has_in = pass > 0 || (seg & 1u);                                   \
         in_b = pass > 0 ? pbnd + ((pass - 1) & 1)                          \
                         : a.seg_bnd + (size_t)off16 * 16 + half;           \
         if (t == 0) {                                                      \
-            dcur = __ldg(a.db + off16);                                    \
-            if (ncols > 8) dnext = __ldg(a.db + off16 + 1);                \
             if (has_in) {                                                  \
                 bq0 = in_b[0];                                             \
                 if (ncols > 1) bq1 = in_b[2];                              \
@@ -227,23 +227,18 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
     }
 
     while (!__all_sync(FULL, done)) {
-        uint32_t d_in = __shfl_up_sync(FULL, d_out, 1, T);
         uint32_t h_in = __shfl_up_sync(FULL, out_h, 1, T);
         uint32_t f_in = __shfl_up_sync(FULL, out_f, 1, T);
+        const uint32_t d_in = d_cur;           // this thread's top column, loaded a step ahead
+        {
+            const int c1 = s + 1 - 2 * t;
+            d_cur = (c1 >= 0 && c1 < ncols) ? (((uint32_t)__ldg(col + c1) >> (8 * half)) & 0xffu)
+                                             : (uint32_t)kZeroCode;
+        }
         if (t == 0) {
-            d_in = kZeroCode;
             h_in = Z;
             f_in = Z;
             if (s < ncols) {
-                if (s > 0 && (s & 7) == 0) {
-                    dcur = dnext;
-                    if (s + 8 < ncols) dnext = __ldg(a.db + off16 + (s >> 3) + 1);
-                }
-                d_in = (dcur.x >> (8 * half)) & 0xffu;
-                dcur.x = __funnelshift_r(dcur.x, dcur.y, 16);
-                dcur.y = __funnelshift_r(dcur.y, dcur.z, 16);
-                dcur.z = __funnelshift_r(dcur.z, dcur.w, 16);
-                dcur.w >>= 16;
                 if (has_in) {
                     h_in = bq0.x;
                     f_in = bq0.y;
@@ -294,7 +289,6 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
             }
         }
         prev_h = h_in;
-        d_out = d_bot;
         d_bot = d_in;
         ++s;
         if (!done && s == nsteps) {   // uniform within the group
