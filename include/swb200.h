@@ -375,7 +375,9 @@ sw_status sw_traceback(struct sw_ctx *ctx, const uint8_t *query, uint32_t qlen,
  * stacks as in sw_search_batch; a request joins at the next round boundary
  * and completes after `chunks` rounds with the same hits sw_search gives.
  * While serving, sw_db_load, sw_search, sw_search_device, sw_search_batch
- * and sw_set_stream return SW_ERR_BUSY. */
+ * and sw_set_stream return SW_ERR_BUSY, and the context's error text belongs
+ * to the scheduler thread: a failed request carries its status in
+ * sw_serve_result; read sw_last_error(ctx) after sw_serve_stop. */
 typedef struct sw_serve_options {
     uint32_t max_active;      /* requests in flight on the device (slots) */
     uint32_t chunks;          /* rounds per request: DB chunks of the ring */

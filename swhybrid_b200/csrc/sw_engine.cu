@@ -627,15 +627,6 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
     const sw_kernel_config cfg = choose_config(ctx, qlen);
     ctx->stats.used = cfg;
     *launches = 0;
-    sw_ctx::Marks mk{};
-    sw_status ms = take_marks(ctx, &mk);
-    if (ms != SW_OK) return ms;
-    mk.fp_launches = 0;
-    mk.cells = (uint64_t)qlen * ctx->n_residues;
-    SW_CUDA(ctx, cudaEventRecord(mk.e[0], st));
-    SW_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 16 * sizeof(int), st));
-    SW_CUDA(ctx, cudaMemsetAsync(ctx->d_scores, 0, (size_t)(ctx->n_records + 1) * sizeof(int), st));
-    SW_CUDA(ctx, cudaEventRecord(mk.e[1], st));
     // pairs [0, n_long) are longer than the cut-over
     int64_t n_long = ctx->n_pairs;
     const int cutover = cfg.cutover > 0 ? cfg.cutover : auto_cutover(ctx, cfg, qlen);
@@ -683,6 +674,17 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
                    "query of %d residues does not fit shape %dx%d (profile %zu bytes)", qlen,
                    sg.T, sg.R, k->smem(qlen));
     }
+    // the search's timing events, taken after every check (a refused search
+    // holds none), then its buffers cleared
+    sw_ctx::Marks mk{};
+    sw_status ms = take_marks(ctx, &mk);
+    if (ms != SW_OK) return ms;
+    mk.fp_launches = 0;
+    mk.cells = (uint64_t)qlen * ctx->n_residues;
+    SW_CUDA(ctx, cudaEventRecord(mk.e[0], st));
+    SW_CUDA(ctx, cudaMemsetAsync(ctx->d_counters, 0, 16 * sizeof(int), st));
+    SW_CUDA(ctx, cudaMemsetAsync(ctx->d_scores, 0, (size_t)(ctx->n_records + 1) * sizeof(int), st));
+    SW_CUDA(ctx, cudaEventRecord(mk.e[1], st));
     int reserved_sms = 0;
     if (split) {
         uint64_t long_cols = 0;

@@ -54,7 +54,7 @@ def free_port():
 
 def test_two_rank_merge_equals_whole_db():
     world = 2
-    with mp.Manager() as m:
+    with mp.get_context("spawn").Manager() as m:
         out = m.dict()
         mp.spawn(worker, args=(world, free_port(), out), nprocs=world, join=True)
         got = dict(out)
