@@ -14,7 +14,7 @@
 //   op 6  three-input integer add (IADD3)
 //   op 7  three-input logic op (LOP3)
 //   op 8  the first pass's per-row cell recurrence as sw_wavefront.cuh runs
-//         it (4 DPX + 1 IMAD + 1 PRMT per row, 1 three-way max per two rows),
+//         it (4 DPX + 1 32-bit add + 1 PRMT per row, 1 three-way max per two rows),
 //         without its shared-memory loads and shuffles
 //   op 9  __hmax2 (half2 max), op 10 __hadd2, op 11 __hmax2 and
 //         __viaddmax_s16x2 interleaved 1:1 (does half2 max use another pipe?)
@@ -123,7 +123,7 @@ __global__ void __launch_bounds__(512) cell2_kernel(uint32_t* sink, int iters, u
     constexpr int R = 16;
     uint32_t H[R], E[R];
     const uint32_t tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t Z = 0x000c000cu, NQ = 0u - Z, NE = 0xfffefffeu, one = seed >> 31 | 1u;
+    const uint32_t Z = 0x000c000cu, NQ = 0u - Z, NE = 0xfffefffeu;
 #pragma unroll
     for (int k = 0; k < R; ++k) {
         H[k] = Z + ((tid + k) & 0x000f000fu);
@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(512) cell2_kernel(uint32_t* sink, int iters, u
             h = __vimax3_s16x2(h, f, Z);
             diag = H[k];
             H[k] = h;
-            const uint32_t hq = mad(h, one, NQ);
+            const uint32_t hq = h + NQ;
             E[k] = __viaddmax_s16x2(E[k], NE, hq);
             f = __viaddmax_s16x2(f, NE, hq);
             if (k & 1) S = __vimax3_s16x2(S, H[k - 1], H[k]);

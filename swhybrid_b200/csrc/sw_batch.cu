@@ -227,7 +227,6 @@ sw_status enqueue_batch(sw_ctx* ctx, sw_batch_state* b, uint32_t nq, size_t qbyt
             q.bias2 |= q.bias2 << 16;
             q.neg_e = (uint32_t)(uint16_t)(int16_t)(-ctx->params.gap_extend);
             q.neg_e |= q.neg_e << 16;
-            q.one = 1u;
             q.bnd = b->d_bnd + b->bnd_cap / 2;
             q.bnd_group = L.bnd_group;
             q.scores = b->d_scores;
@@ -262,7 +261,6 @@ sw_status enqueue_batch(sw_ctx* ctx, sw_batch_state* b, uint32_t nq, size_t qbyt
         a.bias2 |= a.bias2 << 16;
         a.neg_e = (uint32_t)(uint16_t)(int16_t)(-ctx->params.gap_extend);
         a.neg_e |= a.neg_e << 16;
-        a.one = 1u;
         a.bnd = L.long_part ? b->d_bnd : b->d_bnd + b->bnd_cap / 2;
         a.bnd_group = L.bnd_group;
         a.scores = b->d_scores;

@@ -38,7 +38,6 @@ struct WfArgs {
     const int8_t* mat;          // 32x32, [query code][db code]; codes >= 24 score 0
     uint32_t bias2;             // dup16(open+extend): the biased zero of a lane
     uint32_t neg_e;             // dup16(-extend)
-    uint32_t one;               // 1 (multiplier of the IMAD subtraction)
     int* counter;               // pairs claimed (zero before the launch)
     uint2* bnd;                 // boundary rows: 16 entries per 16-byte stream unit
     int* scores;                // per sorted record position
@@ -67,7 +66,6 @@ struct BatchArgs {
     const int8_t* mat;
     uint32_t bias2;
     uint32_t neg_e;
-    uint32_t one;
     uint2* bnd;                 // per-group boundary rows
     size_t bnd_group;           // entries per group (2 per column of the longest pair)
     int* scores;                // [query][sorted position], zero before (atomicMax)

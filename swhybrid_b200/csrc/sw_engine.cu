@@ -718,7 +718,6 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
         la.bias2 |= la.bias2 << 16;
         la.neg_e = (uint32_t)(uint16_t)(int16_t)(-ctx->params.gap_extend);
         la.neg_e |= la.neg_e << 16;
-        la.one = 1u;
         la.scores = ctx->d_scores;
         la.n_records = (int)ctx->n_records;
         la.ovf_list = ctx->d_ovf;
@@ -755,7 +754,6 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
         a.mat = ctx->d_mat;
         a.bias2 = (uint32_t)(ctx->params.gap_open + ctx->params.gap_extend);
         a.bias2 |= a.bias2 << 16;
-        a.one = 1u;
         a.neg_e = (uint32_t)(uint16_t)(int16_t)(-ctx->params.gap_extend);
         a.neg_e |= a.neg_e << 16;
         a.counter = ctx->d_counters + sg.counter;

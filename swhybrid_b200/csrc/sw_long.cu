@@ -73,7 +73,6 @@ __global__ void __launch_bounds__(LongBlock<R>::value, 1) sw_long(const LongArgs
     K.bias2 = a.bias2;
     K.neg_q2 = 0u - a.bias2;
     K.neg_e2 = a.neg_e;
-    K.one = a.one;
     const uint32_t Z = a.bias2;
     const int bias = (int)(a.bias2 & 0xffffu);
     const uint2* const prof_p = prof + (w * NJ) * JSTRIDE + t;

@@ -21,7 +21,7 @@ struct LongArgs {
     int qlen;                   // at most kLongMaxPasses * 32 * R rows
     int passes;                 // ceil(qlen / (32 R)); blockDim.x = 32 * passes * pipelines
     const int8_t* mat;
-    uint32_t bias2, neg_e, one; // (open+extend) x2, (-extend) x2, 1
+    uint32_t bias2, neg_e;      // (open+extend) x2, (-extend) x2
     int* scores;                // by sorted position
     int n_records;
     int* ovf_list;              // positions whose 16-bit lanes may have wrapped

@@ -42,7 +42,7 @@ struct QpArgs {
     int nstacks;
     int* counters;              // one unit counter per double stack (zero before)
     const int8_t* mat;
-    uint32_t bias2, neg_e, one;
+    uint32_t bias2, neg_e;
     uint2* bnd;                 // per-group boundary rows
     size_t bnd_group;
     int* scores;                // [query][sorted position], zero before (atomicMax)
@@ -146,7 +146,6 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
     K.bias2 = a.bias2;
     K.neg_q2 = 0u - a.bias2;
     K.neg_e2 = a.neg_e;
-    K.one = a.one;
     const uint32_t Z = a.bias2;
     const int bias = (int)(a.bias2 & 0xffffu);
     const int units = 2 * a.pair_count;

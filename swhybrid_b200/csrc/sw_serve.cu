@@ -257,7 +257,6 @@ sw_status run_round(sw_ctx* ctx, sw_serve_state* s, int chunk, std::vector<int>&
         a.bias2 |= a.bias2 << 16;
         a.neg_e = (uint32_t)(uint16_t)(int16_t)(-ctx->params.gap_extend);
         a.neg_e |= a.neg_e << 16;
-        a.one = 1u;
         a.bnd = s->d_bnd;
         a.bnd_group = s->bnd_group;
         a.scores = s->d_scores;

@@ -71,15 +71,6 @@ __device__ __forceinline__ uint32_t pack_row(int i, const uint2& A, const uint2&
     }
 }
 
-// 32-bit integer multiply-add (kept as IMAD: the multiplier is a run-time 1),
-// used for the packed subtraction h - (open+extend) on lanes that are biased so
-// that no half can borrow from the other.
-__device__ __forceinline__ uint32_t mad_u32(uint32_t a, uint32_t b, uint32_t c) {
-    uint32_t r;
-    asm("mad.lo.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(a), "r"(b), "r"(c));
-    return r;
-}
-
 // Constants of the cell recurrence.  Every H/E/F/S lane holds value + B with
 // B = open+extend (so "score 0" is B): h' >= B keeps h' - (open+extend) >= 0
 // in both halves, which makes the packed subtraction an ordinary 32-bit add.
@@ -87,7 +78,6 @@ struct CellK {
     uint32_t bias2;     // (B, B)
     uint32_t neg_q2;    // -(B << 16 | B) mod 2^32, i.e. subtract open+extend per half
     uint32_t neg_e2;    // (-extend, -extend)
-    uint32_t one;       // 1, from a kernel argument
 };
 
 // Row k's profile word from a chunk pair (A: record 2p's residue, B: record
@@ -131,7 +121,7 @@ __device__ __forceinline__ void forward_cell(uint32_t& Hk, uint32_t& Ek, uint32_
                                              const CellK& K) {
     const uint32_t h = __vimax3_s16x2(Hk, f, K.bias2);
     Hk = h;
-    const uint32_t hq = mad_u32(h, K.one, K.neg_q2);
+    const uint32_t hq = h + K.neg_q2;
     Ek = __viaddmax_s16x2(Ek, K.neg_e2, hq);
     f = __viaddmax_s16x2(f, K.neg_e2, hq);
 }
@@ -176,7 +166,7 @@ struct RunArgs {
     int pair_count;
     int* counter;               // pairs of the range claimed so far
     int P;                      // query passes of T*R rows
-    uint32_t bias2, neg_e, one; // see CellK
+    uint32_t bias2, neg_e;      // see CellK
     uint2* bnd;                 // boundary rows between passes
     size_t bnd_group;           // 0: per-pair rows at bnd + 16*off16; else this many
                                 // entries per group at bnd + group * bnd_group
@@ -218,7 +208,6 @@ __device__ __forceinline__ void run_pairs(const RunArgs& a, const uint2* prof) {
     K.bias2 = a.bias2;
     K.neg_q2 = 0u - a.bias2;
     K.neg_e2 = a.neg_e;
-    K.one = a.one;
     const uint32_t Z = a.bias2;        // biased zero of both lanes
     const int bias = (int)(a.bias2 & 0xffffu);
     const int pair_count = a.pair_count;
@@ -454,7 +443,6 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
     r.P = P;
     r.bias2 = a.bias2;
     r.neg_e = a.neg_e;
-    r.one = a.one;
     r.bnd = a.bnd;
     r.bnd_group = 0;
     r.scores = a.scores;
@@ -494,7 +482,6 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_batch(const BatchArgs a) {
         r.P = P;
         r.bias2 = a.bias2;
         r.neg_e = a.neg_e;
-        r.one = a.one;
         r.bnd = a.bnd;
         r.bnd_group = a.bnd_group;
         r.scores = a.scores;
