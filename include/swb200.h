@@ -69,7 +69,8 @@ typedef struct sw_hit {
  * kept in registers per thread (an even number).  Pairs of records with more
  * than cutover columns run concurrently in the long-pair kernel, whose query
  * passes are pipelined across the warps of a block: the long shape's rows per
- * thread when it is 32 x {8, 16, 24, 32, 64}, otherwise chosen automatically.
+ * thread when it is 32 x {8, 16, 24, 32, 64} and differs from the short shape,
+ * otherwise chosen automatically (the smallest row count of at most 3 passes).
  * The rest use the short shape.  cutover 0: automatic (a split only when the
  * DB's longest pairs would dominate the bulk launch, else one shape -- the
  * long one -- for the whole DB).  sw_run_stats.used reports what ran. */

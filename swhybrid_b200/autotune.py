@@ -13,6 +13,7 @@ them with SW_ERR_UNSUPPORTED).
 from __future__ import annotations
 
 import argparse
+import bisect
 import json
 import os
 import time
@@ -75,15 +76,67 @@ def sweep(ctx: capi.Context, lengths, shapes=None, reps: int = 2, log=print,
     return results
 
 
-def table_from_sweep(results) -> list:
-    """[(max_qlen, (T, R, T, R, 0)), ...]: each measured length covers the
-    lengths up to the midpoint (geometric) to the next measured length."""
+def rows_used(T: int, R: int, qlen: int) -> int:
+    """Query rows a shape computes for a query: whole passes of T*R rows."""
+    return -(-qlen // (T * R)) * T * R
+
+
+def predict_gcups(results, shape: str, qlen: int) -> float | None:
+    """GCUPS of a shape at any query length from the sweep: a shape's rate on
+    the rows it computes (measured GCUPS x rows computed / qlen) changes slowly
+    with the length, while the share of those rows that are padding changes
+    at every pass boundary.  The rate is interpolated (in log length) between
+    the two measured lengths around qlen; None if the shape was not measured
+    at both (its profile did not fit) or qlen is far past the last one."""
+    T, R = (int(x) for x in shape.split("x"))
     Ls = sorted(results)
+
+    def rate(L):
+        g = results[L]["all"].get(shape)
+        return None if g is None else g * rows_used(T, R, L) / L
+
+    if qlen <= Ls[0]:
+        r = rate(Ls[0])
+    elif qlen >= Ls[-1]:
+        r = rate(Ls[-1]) if qlen <= 1.5 * Ls[-1] else None
+    else:
+        i = bisect.bisect_left(Ls, qlen)        # Ls[i - 1] < qlen <= Ls[i]
+        r0, r1 = rate(Ls[i - 1]), rate(Ls[i])
+        if r0 is None or r1 is None:
+            return None
+        w = (np.log(qlen) - np.log(Ls[i - 1])) / (np.log(Ls[i]) - np.log(Ls[i - 1]))
+        r = r0 * (1 - w) + r1 * w
+    return None if r is None else r * qlen / rows_used(T, R, qlen)
+
+
+def table_from_sweep(results, step: int = 8, top: int = 8192) -> list:
+    """[(max_qlen, (T, R, T, R, cutover)), ...]: the shape with the best
+    predicted GCUPS (predict_gcups) on a grid of query lengths, runs of equal
+    choices merged.  The cut-over is the one measured with that shape at the
+    nearest measured length when the shape was the best there, else 0 (the
+    library's automatic rule)."""
+    Ls = sorted(results)
+    shapes = sorted({s for L in Ls for s in results[L]["all"]})
     out = []
-    for i, L in enumerate(Ls):
-        hi = int(np.sqrt(L * Ls[i + 1])) if i + 1 < len(Ls) else 1 << 30
-        T, R = (int(x) for x in results[L]["best"].split("x"))
-        out.append((hi, (T, R, T, R, int(results[L].get("cutover", 0)))))
+    for q in range(step, top + step, step):
+        best, bg = None, -1.0
+        for s in shapes:
+            g = predict_gcups(results, s, q)
+            if g is not None and g > bg:
+                best, bg = s, g
+        if best is None:
+            continue
+        near = min(Ls, key=lambda L: abs(np.log(L) - np.log(q)))
+        cut = int(results[near].get("cutover", 0)) if results[near]["best"] == best else 0
+        T, R = (int(x) for x in best.split("x"))
+        cfg = (T, R, T, R, cut)
+        if out and out[-1][1] == cfg:
+            out[-1] = (q, cfg)
+        else:
+            out.append((q, cfg))
+    if out:
+        T, R = (int(x) for x in results[Ls[-1]]["best"].split("x"))
+        out.append((1 << 30, (T, R, T, R, int(results[Ls[-1]].get("cutover", 0)))))
     return out
 
 

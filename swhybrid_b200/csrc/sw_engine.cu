@@ -560,9 +560,10 @@ sw_status take_marks(sw_ctx* ctx, sw_ctx::Marks* m) {
 }
 
 // Cut-over for a configuration without one: a DB whose longest pair needs more
-// than twice the column steps an evenly loaded bulk group gets (the bulk
-// launch would end on a few serial chains) sends the pairs above a quarter of
-// that share to the long-pair kernel; otherwise no split.
+// column steps than an evenly loaded bulk group gets (the bulk launch would end
+// on a few serial chains: groups claim pairs longest first, so below that the
+// long pairs finish inside the share) sends the pairs above a quarter of the
+// share to the long-pair kernel; otherwise no split.
 int auto_cutover(sw_ctx* ctx, const sw_kernel_config& cfg, int qlen) {
     if (ctx->n_pairs == 0) return 0;
     const WfKernel* k = find_kernel(cfg.short_group_width, cfg.short_rows_per_thread);
@@ -570,13 +571,14 @@ int auto_cutover(sw_ctx* ctx, const sw_kernel_config& cfg, int qlen) {
     const int occ = std::max(1, shape_occupancy(ctx, *k, qlen));
     const double groups = (double)occ * ctx->num_sms * (k->block / k->T);
     const double share = (double)ctx->pair_cols_total / groups;
-    if ((double)ctx->pair_ncols[0] <= 2.0 * share) return 0;
+    if ((double)ctx->pair_ncols[0] <= share) return 0;
     return std::max(1024, (int)(share / 4));
 }
 
-// The long-pair kernel for a query: the configured long shape when it is a
-// compiled sw_long row count (group width 32) whose passes fit one pipeline,
-// else the smallest row count that needs at most 3 passes (measured on B200:
+// The long-pair kernel for a query: the configured long shape when the
+// configuration names one apart from the bulk shape (a shape table names one
+// shape for both) and it is a compiled sw_long row count (group width 32)
+// whose passes fit one pipeline, else the smallest row count that needs at most 3 passes (measured on B200:
 // 2-3 passes per pair balance pipeline parallelism against per-step
 // overhead), else at most kLongMaxPasses.  A block takes a whole SM:
 // *pipelines is how many pipelines of *passes warps fit its registers and
@@ -611,7 +613,9 @@ const LongKernel* choose_long(sw_ctx* ctx, const sw_kernel_config& cfg, int qlen
         *smem_bytes = dyn;
         return true;
     };
-    if (cfg.long_group_width == 32)
+    const bool named = cfg.long_group_width != cfg.short_group_width ||
+                       cfg.long_rows_per_thread != cfg.short_rows_per_thread;
+    if (named && cfg.long_group_width == 32)
         for (int i = 0; i < n; ++i)
             if (lk[i].R == cfg.long_rows_per_thread && fits(lk[i])) return &lk[i];
     for (int i = 0; i < n; ++i)

@@ -427,6 +427,246 @@ __device__ __forceinline__ void run_pairs(const RunArgs& a, const uint2* prof) {
 #undef SWB_START_PASS
 }
 
+// Streaming group loop of the plain search.  run_pairs drains the group's
+// wavefront at the end of every pass (2T-1 steps in which part of the group
+// idles), which costs 9 % of the steps at T = 16 on a DB of ~350-residue
+// records and 18 % at T = 32.  Here each thread moves on to the group's next
+// segment (the next pass of the pair, or the next pair) as soon as its own
+// columns of the current one are done, so the wavefront fills only once per
+// launch.  Thread t's top half is on column c of a segment at group step
+// G + c + 2t and its bottom half one column behind, so for one step after a
+// switch the two halves work on different segments: the bottom keeps the
+// profile base and boundary-row view the top had a step earlier.
+//   * The pair descriptor (index, stream offset, columns) goes from thread t-1
+//     to thread t by shuffle at t's switch, 2 steps after t-1's.
+//   * A thread's pair maximum is complete one step after its top leaves the
+//     pair's last pass; it travels down the group in a third shuffle (each
+//     thread adds its own), and thread T-1 writes the pair's scores.
+//   * Thread 0 of pass p+1 reads boundary column j at step G' + j - 2 while
+//     thread T-1 of pass p wrote it at step G + 2T - 1 + j, so a segment that
+//     a later pass depends on lasts at least 2T + 2 steps (padding columns of
+//     zero-score residues, which cannot raise a score); every other segment
+//     lasts at least 3 steps, which keeps the descriptor and maximum hand-offs
+//     one segment apart.
+template <int T, int R>
+__device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) {
+    static_assert(R % 2 == 0 && R >= 4, "R");
+    constexpr int NJ = (R + 7) / 8;
+    constexpr int HALF = R / 2;
+    constexpr int SLOTS = GroupShape<T>::SLOTS;
+    constexpr int JSTRIDE = kCodes * SLOTS;
+    constexpr int PSTRIDE = NJ * JSTRIDE;     // profile words per pass
+    constexpr unsigned FULL = 0xffffffffu;
+    const int P = a.P;
+    const int lane = threadIdx.x & 31;
+    const int t = lane & (T - 1);
+    const int slot = lane & (SLOTS - 1);
+    const unsigned gmask = (T == 32) ? FULL : (((1u << T) - 1u) << (lane & ~(T - 1)));
+    CellK K;
+    K.bias2 = a.bias2;
+    K.neg_q2 = 0u - a.bias2;
+    K.neg_e2 = a.neg_e;
+    const uint32_t Z = a.bias2;
+    const int bias = (int)(a.bias2 & 0xffffu);
+    const int pair_count = a.pair_count;
+    const int dep_steps = 2 * T + 2;
+
+    uint32_t H[R], E[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        H[k] = Z;
+        E[k] = Z;
+    }
+    uint32_t S_top = Z, S_bot = Z, S_pend = Z, acc_out = Z;
+    uint32_t out_h = Z, out_f = Z, prev_h = Z, mid_h = Z, mid_f = Z;
+    uint32_t d_bot = kPadPair, d_cur = kPadPair;
+    // the top half's segment
+    int pair = 0, pass = 0, ncols = 0, nst = 0, c = 0;
+    uint32_t off16 = 0u;
+    const unsigned short* col = reinterpret_cast<const unsigned short*>(a.db);
+    const uint2* prof_t = prof + slot;
+    uint2* wrow = a.bnd;       // boundary row this pass writes (thread T-1) ...
+    int wlim = 0;              // ... for columns below this (0: last pass)
+    // the bottom half's view: the top's of the previous step
+    const uint2* prof_b = prof_t;
+    uint2* b_wrow = wrow;
+    int b_wlim = 0, b_col = -1;
+    // a pair whose maximum is being finished
+    int fpair = 0;
+    bool fpend = false, fin = false;
+    // thread 0: the next pair (claimed one pair ahead) and the boundary row
+    // read by passes after the first (two columns prefetched)
+    int next = 0;
+    Pair2 ninfo{0u, 0u};
+    uint2 bq0 = make_uint2(Z, Z), bq1 = bq0;
+    const uint2* rrow = a.bnd;
+
+#define SWS_SET_SEG()                                                          \
+    {                                                                          \
+        nst = ncols > ((pass + 1 < P) ? dep_steps : 3) ? ncols                 \
+                                                       : ((pass + 1 < P) ? dep_steps : 3); \
+        col = reinterpret_cast<const unsigned short*>(a.db) + (size_t)off16 * 8; \
+        uint2* const pb = a.bnd + (size_t)off16 * 16;                          \
+        wrow = pb + (pass & 1);                                                \
+        wlim = (pass + 1 < P) ? ncols : 0;                                     \
+        rrow = pb + ((pass - 1) & 1);                                          \
+        prof_t = prof + pass * PSTRIDE + slot;                                 \
+    }
+
+    {
+        int v = 0;
+        if (t == 0) v = atomicAdd(a.counter, 1);
+        v = __shfl_sync(gmask, v, 0, T);
+        pair = v;
+        if (v < pair_count) {
+            const Pair2 pr = a.pairs[a.pair_begin + v];
+            off16 = pr.off16;
+            ncols = (int)pr.ncols;
+            if (t == 0) next = atomicAdd(a.counter, 1);
+        } else {
+            fin = true;
+        }
+        SWS_SET_SEG()
+        c = -2 * t;
+        d_cur = (t == 0 && ncols > 0) ? (uint32_t)__ldg(col) : kPadPair;
+    }
+
+    while (!__all_sync(FULL, fin)) {
+        if (P > 1) __syncwarp();      // orders the boundary row's stores and loads
+        uint32_t h_in = __shfl_up_sync(FULL, out_h, 1, T);
+        uint32_t f_in = __shfl_up_sync(FULL, out_f, 1, T);
+        const uint32_t acc_in = __shfl_up_sync(FULL, acc_out, 1, T);
+        const uint32_t d_in = d_cur;
+        {
+            const int c1 = c + 1;     // this thread's top column next step
+            d_cur = (c1 >= 0 && c1 < ncols) ? (uint32_t)__ldg(col + c1) : kPadPair;
+        }
+        if (t == 0) {
+            h_in = Z;
+            f_in = Z;
+            if (pass > 0 && c < ncols) {
+                h_in = bq0.x;
+                f_in = bq0.y;
+                bq0 = bq1;
+                if (c + 2 < ncols) bq1 = rrow[2 * (c + 2)];
+            }
+            // the next pair's table entry, once its claim has returned
+            if (pass == 0 && c == (nst < 9 ? nst - 1 : 8) && next < pair_count)
+                ninfo = a.pairs[a.pair_begin + next];
+        }
+        if (!fin && c >= 0) {
+            const uint2* t0 = prof_t + (int)(d_in & 0xffu) * SLOTS;
+            const uint2* t1 = prof_t + (int)((d_in >> 8) & 0xffu) * SLOTS;
+            const uint2* b0 = prof_b + (int)(d_bot & 0xffu) * SLOTS;
+            const uint2* b1 = prof_b + (int)((d_bot >> 8) & 0xffu) * SLOTS;
+            const uint32_t bot_diag = mid_h;
+            uint32_t f_top = f_in, f_bot = mid_f;
+            mid_h = H[HALF - 1];
+            reverse_sweep<R, 0, HALF>(H, E, t0, t1, JSTRIDE, prev_h);
+            reverse_sweep<R, HALF, R>(H, E, b0, b1, JSTRIDE, bot_diag);
+#pragma unroll
+            for (int i = 0; i < HALF; ++i) {
+                forward_cell(H[i], E[i], f_top, K);
+                forward_cell(H[HALF + i], E[HALF + i], f_bot, K);
+                if (i & 1) S_top = __vimax3_s16x2(S_top, H[i - 1], H[i]);
+                if (i & 1) S_bot = __vimax3_s16x2(S_bot, H[HALF + i - 1], H[HALF + i]);
+                if (!(i & 1) && i == HALF - 1) {
+                    S_top = __vimax3_s16x2(S_top, H[i], Z);
+                    S_bot = __vimax3_s16x2(S_bot, H[HALF + i], Z);
+                }
+            }
+            mid_f = f_top;
+            out_h = H[R - 1];
+            out_f = f_bot;
+            if (t == T - 1 && b_col >= 0 && b_col < b_wlim)
+                b_wrow[2 * b_col] = make_uint2(out_h, out_f);
+        }
+        prev_h = h_in;
+        d_bot = d_in;
+        prof_b = prof_t;
+        b_wrow = wrow;
+        b_wlim = wlim;
+        b_col = c;
+        if (fpend) {
+            // the bottom has just done the finished pair's last column: this
+            // thread's maximum joins the group's, thread T-1 holds the result
+            fpend = false;
+            uint32_t m = __vimax3_s16x2(S_pend, S_bot, Z);
+            if (t > 0) m = __vimax3_s16x2(m, acc_in, Z);
+            acc_out = m;
+            S_bot = Z;
+            if (t == T - 1) {
+                const int pos = 2 * (a.pair_begin + fpair);
+                const int s0 = lo16(m), s1 = hi16(m);
+                a.scores[pos] = s0 - bias;
+                if (s0 >= a.ovf_thresh) {
+                    const int j = atomicAdd(a.ovf_count, 1);
+                    if (j < a.ovf_cap) a.ovf_list[j] = a.ovf_base + pos;
+                }
+                if (pos + 1 < a.n_records) {
+                    a.scores[pos + 1] = s1 - bias;
+                    if (s1 >= a.ovf_thresh) {
+                        const int j = atomicAdd(a.ovf_count, 1);
+                        if (j < a.ovf_cap) a.ovf_list[j] = a.ovf_base + pos + 1;
+                    }
+                }
+            }
+            if (pair >= pair_count) fin = true;
+        }
+        if (c == 0) {   // the bottom starts this segment's column 0 next step
+#pragma unroll
+            for (int k = HALF; k < R; ++k) {
+                H[k] = Z;
+                E[k] = Z;
+            }
+        }
+        // the top leaves its segment: set up the next one
+        const bool adv = !fin && c == nst - 1;
+        if (__any_sync(FULL, adv)) {
+            const int up_pair = __shfl_up_sync(FULL, pair, 1, T);
+            const uint32_t up_off = __shfl_up_sync(FULL, off16, 1, T);
+            const int up_ncols = __shfl_up_sync(FULL, ncols, 1, T);
+            if (adv) {
+                if (pass + 1 < P) {
+                    ++pass;
+                } else {
+                    S_pend = S_top;
+                    S_top = Z;
+                    fpair = pair;
+                    fpend = true;
+                    pass = 0;
+                    if (t == 0) {
+                        pair = next;
+                        off16 = ninfo.off16;
+                        ncols = (int)ninfo.ncols;
+                        if (pair < pair_count) next = atomicAdd(a.counter, 1);
+                    } else {
+                        pair = up_pair;
+                        off16 = up_off;
+                        ncols = up_ncols;
+                    }
+                    if (pair >= pair_count) ncols = 0;
+                }
+                SWS_SET_SEG()
+                c = -1;
+#pragma unroll
+                for (int k = 0; k < HALF; ++k) {
+                    H[k] = Z;
+                    E[k] = Z;
+                }
+                prev_h = Z;
+                if (t == 0 && pass > 0) {
+                    if (ncols > 0) bq0 = rrow[0];
+                    if (ncols > 1) bq1 = rrow[2];
+                }
+                d_cur = (ncols > 0) ? (uint32_t)__ldg(col) : kPadPair;
+            }
+        }
+        ++c;
+    }
+#undef SWS_SET_SEG
+}
+
 // Plain search: one query, the pairs of one range.
 template <int T, int R, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
@@ -454,7 +694,7 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
     r.ovf_cap = a.n_records + 1;
     r.pair_ids = nullptr;
     r.rb_map = nullptr;
-    run_pairs<T, R, false>(r, prof);
+    run_stream<T, R>(r, prof);
 }
 
 // Batched search: one persistent launch over a list of query stacks (each

@@ -74,3 +74,28 @@ def test_generators_are_seeded_and_shaped():
     assert counts[param.ALPHABET.index("B")] == 0
     sweep = synth.sweep_lengths()
     assert sweep[0] == 144 and sweep[-1] == 5478 and len(sweep) == 20
+
+
+def test_tuning_table_accounts_for_pass_padding():
+    """The shape table derived from a sweep predicts each shape from its rate on
+    the rows it computes, so a shape whose last pass would be mostly padding
+    loses to one that fits the length, and measured lengths reproduce."""
+    from swhybrid_b200 import autotune
+    rate = {"16x64": 4000.0, "32x56": 4100.0}          # GCUPS on computed rows
+    res = {}
+    for L in (1000, 1500, 2000, 3000):
+        row = {s: rate[s] * L / autotune.rows_used(*map(int, s.split("x")), L) for s in rate}
+        res[L] = {"best": max(row, key=row.get), "cutover": 0, "all": row}
+    for L in res:
+        for s in rate:
+            assert abs(autotune.predict_gcups(res, s, L) - res[L]["all"][s]) < 1e-6
+    tab = autotune.table_from_sweep(res)
+    pick = lambda q: next(cfg for hi, cfg in tab if q <= hi)[:2]
+    assert pick(1792) == (32, 56)       # one full 1,792-row pass
+    assert pick(1900) == (16, 64)       # 2 x 1,024 rows, not 2 x 1,792
+    assert pick(3584) == (32, 56)
+    assert [hi for hi, _ in tab] == sorted(hi for hi, _ in tab)
+    committed = autotune.load_table()
+    assert committed and [hi for hi, _ in committed] == sorted(hi for hi, _ in committed)
+    shapes = set(capi.shapes())
+    assert all((c[0], c[1]) in shapes and (c[2], c[3]) in shapes for _, c in committed)

@@ -97,6 +97,32 @@ def test_cutover_split_bit_exact(ctx):
         ctx.set_kernel_config(None)
 
 
+def test_streamed_segments_short_and_empty_records(ctx):
+    """The plain kernel's groups stream from pass to pass and pair to pair
+    without draining the wavefront.  Records of 0..80 residues (pairs shorter
+    than the 2T+2 steps a pass that the next one depends on is padded to, runs
+    of empty records) under a query of several passes for every group width,
+    and DBs with fewer pairs than thread groups, against the oracle."""
+    rng = np.random.default_rng(41)
+    q = synth.residues(rng, 700)
+    lens = rng.integers(0, 81, size=900)
+    lens[::37] = 0
+    lens[100:106] = 0
+    big = synth.db_from_lengths(rng, lens)
+    big, _ = synth.plant_homologs(rng, big, q, 0.02)
+    dbs = [big] + [synth.db_from_lengths(rng, np.array(l)) for l in ([5], [0, 70], [66, 1, 2], [700, 3, 0, 64, 65])]
+    wants = [oracle.search(q, d.residues, d.offsets, M, 12, 2) for d in dbs]
+    try:
+        for d, want in zip(dbs, wants):
+            ctx.load_db(d.residues, d.offsets)
+            for T, R in [(4, 8), (8, 12), (16, 6), (16, 48), (32, 4), (32, 10), (32, 40)]:
+                ctx.set_kernel_config((T, R, T, R, 0))
+                _, scores = ctx.search(q, want_scores=True)
+                np.testing.assert_array_equal(scores, want, err_msg=f"{T}x{R} n={d.n}")
+    finally:
+        ctx.set_kernel_config(None)
+
+
 def test_int16_threshold_and_int32_pass():
     """Scores around the 16-bit overflow threshold and above 65535: the 32-bit
     re-score must be exact; the reference cap reports 65535."""
