@@ -128,7 +128,14 @@ __device__ __forceinline__ void reverse_sweep_qp(uint32_t (&H)[R], const uint32_
 }
 
 // One double stack: every group claims units (records) and scores them
-// against both lanes' stacks.  Returns when the units are exhausted.
+// against both lanes' stacks.  Returns when the units are exhausted.  The
+// groups stream from pass to pass and unit to unit without draining, as in
+// run_stream (sw_wavefront.cuh), with the maximum chain and the last-thread
+// atomicMax done per lane (each lane has its own query map).  Rows above pass
+// 0 come from seg_bnd when the stack continues an earlier segment (bit 0 of
+// seg), and the last pass writes its last row there for the next segment
+// (bit 1): a column is read (pass 0, thread 0) 2T + 1 steps before the last
+// pass's thread T-1 writes it, so one buffer serves both.
 template <int T, int R>
 __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, int P, int* counter,
                                            const int2* rb_map, uint32_t seg) {
@@ -137,6 +144,7 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
     constexpr int HALF = R / 2;
     constexpr int SLOTS = GroupShape<T>::SLOTS;
     constexpr int JSTRIDE = kCodes * SLOTS;
+    constexpr int PSTRIDE = NJ * JSTRIDE;
     constexpr unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const int t = lane & (T - 1);
@@ -149,118 +157,118 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
     const uint32_t Z = a.bias2;
     const int bias = (int)(a.bias2 & 0xffffu);
     const int units = 2 * a.pair_count;
+    const int dep_steps = 2 * T + 2;
     uint2* const pbnd = a.bnd + (size_t)((blockIdx.x * blockDim.x + threadIdx.x) / T) * a.bnd_group;
 
     uint32_t H[R], E[R];
-    uint32_t S = Z, out_h = Z, out_f = Z, prev_h = Z, mid_h = Z, mid_f = Z;
-    uint32_t d_bot = kZeroCode, d_cur = kZeroCode;
-    const unsigned short* col = reinterpret_cast<const unsigned short*>(a.db);
-    int unit = 0, next = 0, pass = 0, s = 0, nsteps = 0, ncols = 0, half = 0;
-    uint32_t off16 = 0u;
-    bool done = false;
-    uint2 bq0 = make_uint2(Z, Z), bq1 = bq0;
-    Pair2 ninfo{0u, 0u};
-    int q_lo = -1, q_hi = -1;
-    uint32_t reset = 0u;     // lanes whose query starts at this thread's first row
-    bool has_in = false;     // the pass takes its rows above from a boundary row
-    const uint2* in_b = pbnd;
-
-#define SWQ_START_PASS()                                                   \
-    {                                                                      \
-        s = 0;                                                             \
-        const int2 rb = rb_map[pass * T + t];                              \
-        q_lo = rb.x < 0 ? -1 : (rb.x & (kFirstBit - 1));                   \
-        q_hi = rb.y < 0 ? -1 : (rb.y & (kFirstBit - 1));                   \
-        reset = ((rb.x >= 0 && (rb.x & kFirstBit)) ? 0x0000ffffu : 0u) |   \
-                ((rb.y >= 0 && (rb.y & kFirstBit)) ? 0xffff0000u : 0u);    \
-        S = Z;                                                             \
-        nsteps = ncols + 2 * T - 1;                                        \
-        _Pragma("unroll") for (int k = 0; k < R; ++k) {                    \
-            H[k] = Z;                                                      \
-            E[k] = Z;                                                      \
-        }                                                                  \
-        out_h = Z;                                                         \
-        out_f = Z;                                                         \
-        prev_h = Z;                                                        \
-        mid_h = Z;                                                         \
-        mid_f = Z;                                                         \
-        d_bot = kZeroCode;                                                 \
-        col = reinterpret_cast<const unsigned short*>(a.db) + (size_t)off16 * 8; \
-        d_cur = (t == 0 && ncols > 0) ? (((uint32_t)__ldg(col) >> (8 * half)) & 0xffu) \
-                                      : (uint32_t)kZeroCode;               \
-        has_in = pass > 0 || (seg & 1u);                                   \
-        in_b = pass > 0 ? pbnd + ((pass - 1) & 1)                          \
-                        : a.seg_bnd + (size_t)off16 * 16 + half;           \
-        if (t == 0) {                                                      \
-            if (has_in) {                                                  \
-                bq0 = in_b[0];                                             \
-                if (ncols > 1) bq1 = in_b[2];                              \
-            }                                                              \
-        }                                                                  \
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        H[k] = Z;
+        E[k] = Z;
     }
-#define SWQ_TAKE_UNIT(v)                                                   \
-    {                                                                      \
-        if ((v) >= units) {                                                \
-            done = true;                                                   \
-            ncols = 0;                                                     \
-            nsteps = 0;                                                    \
-        } else {                                                           \
-            unit = (v);                                                    \
-            half = unit & 1;                                               \
-            pass = 0;                                                      \
-            if (t == 0) next = atomicAdd(counter, 1);                      \
-            SWQ_START_PASS()                                               \
-        }                                                                  \
+    uint32_t S_top = Z, S_bot = Z, S_pend = Z, acc_out = Z;
+    uint32_t out_h = Z, out_f = Z, prev_h = Z, mid_h = Z, mid_f = Z;
+    uint32_t d_bot = kZeroCode, d_cur = kZeroCode;
+    // the top half's segment
+    int unit = 0, half = 0, pass = 0, ncols = 0, nst = 0, c = 0;
+    uint32_t off16 = 0u;
+    const unsigned short* col = reinterpret_cast<const unsigned short*>(a.db);
+    const uint4* prof_t = prof + slot;
+    uint2* wrow = pbnd;        // where thread T-1 writes the last row ...
+    int wlim = 0;              // ... for columns below this (0: nowhere)
+    int q_lo = -1, q_hi = -1;
+    uint32_t reset = 0u;       // lanes whose query starts at this thread's first row
+    uint32_t last = 0u;        // lanes whose query's rows end at this thread's last row
+    // the bottom half's view: the top's of the previous step
+    const uint4* prof_b = prof_t;
+    uint2* b_wrow = wrow;
+    int b_wlim = 0, b_col = -1;
+    // a segment whose maxima are being finished
+    int f_unit = 0, fq_lo = -1, fq_hi = -1;
+    uint32_t f_reset = 0u, f_last = 0u;
+    bool fpend = false, fin = false;
+    // thread 0: the next unit (claimed one unit ahead) and the rows above
+    int next = 0;
+    Pair2 ninfo{0u, 0u};
+    uint2 bq0 = make_uint2(Z, Z), bq1 = bq0;
+    bool has_in = false;
+    const uint2* rrow = pbnd;
+
+#define SWQ_SET_SEG()                                                          \
+    {                                                                          \
+        const int lo = (pass + 1 < P) ? dep_steps : 3;                         \
+        nst = ncols > lo ? ncols : lo;                                         \
+        col = reinterpret_cast<const unsigned short*>(a.db) + (size_t)off16 * 8; \
+        uint2* const sb = a.seg_bnd + (size_t)off16 * 16 + half;               \
+        wrow = (pass + 1 < P) ? pbnd + (pass & 1) : sb;                        \
+        wlim = (pass + 1 < P || (seg & 2u)) ? ncols : 0;                       \
+        has_in = pass > 0 || (seg & 1u);                                       \
+        rrow = pass > 0 ? pbnd + ((pass - 1) & 1) : sb;                        \
+        prof_t = prof + pass * PSTRIDE + slot;                                 \
+        const int2 rb = rb_map[pass * T + t];                                  \
+        const int2 rn = (t + 1 < T) ? rb_map[pass * T + t + 1] : make_int2(-1, -1); \
+        q_lo = rb.x < 0 ? -1 : (rb.x & (kFirstBit - 1));                       \
+        q_hi = rb.y < 0 ? -1 : (rb.y & (kFirstBit - 1));                       \
+        reset = ((rb.x >= 0 && (rb.x & kFirstBit)) ? 0x0000ffffu : 0u) |       \
+                ((rb.y >= 0 && (rb.y & kFirstBit)) ? 0xffff0000u : 0u);        \
+        last = ((rn.x < 0 || (rn.x & kFirstBit)) ? 0x0000ffffu : 0u) |         \
+               ((rn.y < 0 || (rn.y & kFirstBit)) ? 0xffff0000u : 0u);          \
     }
 
     {
         int v = 0;
         if (t == 0) v = atomicAdd(counter, 1);
         v = __shfl_sync(gmask, v, 0, T);
+        unit = v;
         if (v < units) {
             const Pair2 pr = a.pairs[a.pair_begin + (v >> 1)];
             off16 = pr.off16;
             ncols = (int)pr.ncols;
+            half = v & 1;
+            if (t == 0) next = atomicAdd(counter, 1);
+        } else {
+            fin = true;
         }
-        SWQ_TAKE_UNIT(v)
+        SWQ_SET_SEG()
+        c = -2 * t;
+        d_cur = (t == 0 && ncols > 0) ? (((uint32_t)__ldg(col) >> (8 * half)) & 0xffu)
+                                      : (uint32_t)kZeroCode;
+        if (t == 0 && has_in) {
+            if (ncols > 0) bq0 = rrow[0];
+            if (ncols > 1) bq1 = rrow[2];
+        }
     }
 
-    while (!__all_sync(FULL, done)) {
+    while (!__all_sync(FULL, fin)) {
+        __syncwarp();                 // orders the boundary rows' stores and loads
         uint32_t h_in = __shfl_up_sync(FULL, out_h, 1, T);
         uint32_t f_in = __shfl_up_sync(FULL, out_f, 1, T);
-        const uint32_t d_in = d_cur;           // this thread's top column, loaded a step ahead
+        const uint32_t acc_in = __shfl_up_sync(FULL, acc_out, 1, T);
+        const uint32_t d_in = d_cur;
         {
-            const int c1 = s + 1 - 2 * t;
+            const int c1 = c + 1;
             d_cur = (c1 >= 0 && c1 < ncols) ? (((uint32_t)__ldg(col + c1) >> (8 * half)) & 0xffu)
                                              : (uint32_t)kZeroCode;
         }
         if (t == 0) {
             h_in = Z;
             f_in = Z;
-            if (s < ncols) {
-                if (has_in) {
-                    h_in = bq0.x;
-                    f_in = bq0.y;
-                    bq0 = bq1;
-                    if (s + 2 < ncols) bq1 = in_b[2 * (s + 2)];
-                }
-                // the next unit's pair entry, once its claim has returned
-                if (pass == 0 && s == (ncols < 9 ? ncols - 1 : 8) && next < units)
-                    ninfo = a.pairs[a.pair_begin + (next >> 1)];
+            if (has_in && c < ncols) {
+                h_in = bq0.x;
+                f_in = bq0.y;
+                bq0 = bq1;
+                if (c + 2 < ncols) bq1 = rrow[2 * (c + 2)];
             }
+            // the next unit's pair entry, once its claim has returned
+            if (pass == 0 && c == (nst < 9 ? nst - 1 : 8) && next < units)
+                ninfo = a.pairs[a.pair_begin + (next >> 1)];
         }
         // a lane whose query starts here takes nothing from above
         h_in = (h_in & ~reset) | (Z & reset);
         f_in = (f_in & ~reset) | (Z & reset);
-        const int ct = s - 2 * t;
-        const bool top_valid = ct >= 0 && ct < ncols;
-        const bool bot_valid = ct >= 1 && ct <= ncols;
-        if (!done && (ct >= 0 && ct <= ncols)) {
-            const uint32_t wt = top_valid ? d_in : kZeroCode;
-            const uint32_t wb = bot_valid ? d_bot : kZeroCode;
-            const uint4* prof_p = prof + (pass * NJ) * JSTRIDE + slot;
-            const uint4* pt = prof_p + (int)wt * SLOTS;
-            const uint4* pb = prof_p + (int)wb * SLOTS;
+        if (!fin && c >= 0) {
+            const uint4* pt = prof_t + (int)d_in * SLOTS;
+            const uint4* pb = prof_b + (int)d_bot * SLOTS;
             const uint32_t bot_diag = mid_h;
             uint32_t f_top = f_in, f_bot = mid_f;
             mid_h = H[HALF - 1];
@@ -270,55 +278,45 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
             for (int i = 0; i < HALF; ++i) {
                 forward_cell(H[i], E[i], f_top, K);
                 forward_cell(H[HALF + i], E[HALF + i], f_bot, K);
-                if (i & 1) S = __vimax3_s16x2(S, H[i - 1], H[i]);
-                if (i & 1) S = __vimax3_s16x2(S, H[HALF + i - 1], H[HALF + i]);
-                if (!(i & 1) && i == HALF - 1) S = __vimax3_s16x2(S, H[i], H[HALF + i]);
+                if (i & 1) S_top = __vimax3_s16x2(S_top, H[i - 1], H[i]);
+                if (i & 1) S_bot = __vimax3_s16x2(S_bot, H[HALF + i - 1], H[HALF + i]);
             }
             mid_f = f_top;
-            if (bot_valid) {
-                out_h = H[R - 1];
-                out_f = f_bot;
-                if (t == T - 1) {
-                    if (pass + 1 < P)
-                        pbnd[2 * (ct - 1) + (pass & 1)] = make_uint2(out_h, out_f);
-                    else if (seg & 2u)
-                        a.seg_bnd[(size_t)off16 * 16 + 2 * (ct - 1) + half] =
-                            make_uint2(out_h, out_f);
-                }
-            }
+            out_h = H[R - 1];
+            out_f = f_bot;
+            if (t == T - 1 && b_col >= 0 && b_col < b_wlim)
+                b_wrow[2 * b_col] = make_uint2(out_h, out_f);
         }
         prev_h = h_in;
         d_bot = d_in;
-        ++s;
-        if (!done && s == nsteps) {   // uniform within the group
-            __syncwarp(gmask);
-            // per lane: segmented max over the threads of each query of this
-            // pass; the segment's first thread adds it to the query's score
-#pragma unroll
-            for (int o = 1; o < T; o <<= 1) {
-                const uint32_t v = __shfl_down_sync(gmask, S, o, T);
-                const int vlo = __shfl_down_sync(gmask, q_lo, o, T);
-                const int vhi = __shfl_down_sync(gmask, q_hi, o, T);
-                uint32_t m = 0u;
-                if (t + o < T) m = (vlo == q_lo ? 0x0000ffffu : 0u) | (vhi == q_hi ? 0xffff0000u : 0u);
-                S = __vimax3_s16x2(S, (v & m) | (Z & ~m), Z);
-            }
-            const int gp = a.pair_ids ? (int)a.pair_ids[a.pair_begin + (unit >> 1)]
-                                      : a.pair_begin + (unit >> 1);
-            const int pos = 2 * gp + half;
+        prof_b = prof_t;
+        b_wrow = wrow;
+        b_wlim = wlim;
+        b_col = c;
+        if (fpend) {
+            // the bottom has just done the finished segment's last column:
+            // per lane, this thread's maximum joins its query's chain
+            fpend = false;
+            uint32_t m = __vimax3_s16x2(S_pend, S_bot, Z);
+            const uint32_t cont = (t > 0) ? ~f_reset : 0u;
+            m = __vimax3_s16x2(m, (acc_in & cont) | (Z & ~cont), Z);
+            acc_out = m;
+            const int gp = a.pair_ids ? (int)a.pair_ids[a.pair_begin + (f_unit >> 1)]
+                                      : a.pair_begin + (f_unit >> 1);
+            const int pos = 2 * gp + (f_unit & 1);
             if (pos < a.n_records) {
-                if (q_lo >= 0 && ((reset & 0xffffu) || t == 0)) {
-                    const int s0 = lo16(S);
-                    const int qb = q_lo * a.n_records;
+                if (fq_lo >= 0 && (f_last & 0xffffu)) {
+                    const int s0 = lo16(m);
+                    const int qb = fq_lo * a.n_records;
                     atomicMax(a.scores + qb + pos, s0 - bias);
                     if (s0 >= a.ovf_thresh) {
                         const int j = atomicAdd(a.ovf_count, 1);
                         if (j < a.ovf_cap) a.ovf_list[j] = qb + pos;
                     }
                 }
-                if (q_hi >= 0 && ((reset >> 16) || t == 0)) {
-                    const int s1 = hi16(S);
-                    const int qb = q_hi * a.n_records;
+                if (fq_hi >= 0 && (f_last >> 16)) {
+                    const int s1 = hi16(m);
+                    const int qb = fq_hi * a.n_records;
                     atomicMax(a.scores + qb + pos, s1 - bias);
                     if (s1 >= a.ovf_thresh) {
                         const int j = atomicAdd(a.ovf_count, 1);
@@ -326,19 +324,66 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
                     }
                 }
             }
-            if (pass + 1 < P) {
-                ++pass;
-                SWQ_START_PASS()
-            } else {
-                const int v = __shfl_sync(gmask, next, 0, T);
-                off16 = __shfl_sync(gmask, ninfo.off16, 0, T);
-                ncols = (int)__shfl_sync(gmask, ninfo.ncols, 0, T);
-                SWQ_TAKE_UNIT(v)
+            S_bot = Z;
+            if (unit >= units) fin = true;
+        }
+        if (c == 0) {   // the bottom starts this segment's column 0 next step
+#pragma unroll
+            for (int k = HALF; k < R; ++k) {
+                H[k] = Z;
+                E[k] = Z;
             }
         }
+        const bool adv = !fin && c == nst - 1;
+        if (__any_sync(FULL, adv)) {
+            const int up_unit = __shfl_up_sync(FULL, unit, 1, T);
+            const uint32_t up_off = __shfl_up_sync(FULL, off16, 1, T);
+            const int up_ncols = __shfl_up_sync(FULL, ncols, 1, T);
+            if (adv) {
+                S_pend = S_top;
+                S_top = Z;
+                f_unit = unit;
+                fq_lo = q_lo;
+                fq_hi = q_hi;
+                f_reset = reset;
+                f_last = last;
+                fpend = true;
+                if (pass + 1 < P) {
+                    ++pass;
+                } else {
+                    pass = 0;
+                    if (t == 0) {
+                        unit = next;
+                        off16 = ninfo.off16;
+                        ncols = (int)ninfo.ncols;
+                        if (unit < units) next = atomicAdd(counter, 1);
+                    } else {
+                        unit = up_unit;
+                        off16 = up_off;
+                        ncols = up_ncols;
+                    }
+                    if (unit >= units) ncols = 0;
+                    half = unit & 1;
+                }
+                SWQ_SET_SEG()
+                c = -1;
+#pragma unroll
+                for (int k = 0; k < HALF; ++k) {
+                    H[k] = Z;
+                    E[k] = Z;
+                }
+                prev_h = Z;
+                if (t == 0 && has_in) {
+                    if (ncols > 0) bq0 = rrow[0];
+                    if (ncols > 1) bq1 = rrow[2];
+                }
+                d_cur = (ncols > 0) ? (((uint32_t)__ldg(col) >> (8 * half)) & 0xffu)
+                                    : (uint32_t)kZeroCode;
+            }
+        }
+        ++c;
     }
-#undef SWQ_TAKE_UNIT
-#undef SWQ_START_PASS
+#undef SWQ_SET_SEG
 }
 
 // The paired-query batched kernel: blocks walk the double stacks in order.

@@ -158,7 +158,7 @@ __device__ __forceinline__ void build_profile(uint2* prof, const uint8_t* query,
     }
 }
 
-// What one call of run_pairs works on.
+// What one call of run_stream works on.
 struct RunArgs {
     const uint4* db;            // pair column streams
     const Pair2* pairs;         // pair table, ncols descending
@@ -189,269 +189,38 @@ struct RunArgs {
 
 
 // The group loop: every group of T threads claims pairs from the range and
-// scores them against the query whose profile is in prof.  Returns when the
-// range is exhausted (warp-wide).
-template <int T, int R, bool STACKED>
-__device__ __forceinline__ void run_pairs(const RunArgs& a, const uint2* prof) {
-    static_assert(R % 2 == 0 && R >= 4, "R");
-    constexpr int NJ = (R + 7) / 8;    // 8-row profile chunks per thread (last one partial)
-    constexpr int HALF = R / 2;
-    constexpr int SLOTS = GroupShape<T>::SLOTS;
-    constexpr int JSTRIDE = kCodes * SLOTS;
-    constexpr unsigned FULL = 0xffffffffu;
-    const int P = a.P;
-    const int lane = threadIdx.x & 31;
-    const int t = lane & (T - 1);
-    const int slot = lane & (SLOTS - 1);
-    const unsigned gmask = (T == 32) ? FULL : (((1u << T) - 1u) << (lane & ~(T - 1)));
-    CellK K;
-    K.bias2 = a.bias2;
-    K.neg_q2 = 0u - a.bias2;
-    K.neg_e2 = a.neg_e;
-    const uint32_t Z = a.bias2;        // biased zero of both lanes
-    const int bias = (int)(a.bias2 & 0xffffu);
-    const int pair_count = a.pair_count;
-    uint2* const grp_bnd =
-        a.bnd + (size_t)((blockIdx.x * blockDim.x + threadIdx.x) / T) * a.bnd_group;
-
-    // rows [0, HALF): top half, on column s - 2t; rows [HALF, R): bottom half,
-    // on column s - 2t - 1 (s = step within the pass)
-    uint32_t H[R], E[R];
-    uint32_t S = Z;
-    uint32_t out_h = Z, out_f = Z, prev_h = Z, mid_h = Z, mid_f = Z;
-    uint32_t d_bot = kPadPair, d_cur = kPadPair;
-    const unsigned short* col = reinterpret_cast<const unsigned short*>(a.db);
-    int pair = 0, next = 0, pass = 0, s = 0, nsteps = 0, ncols = 0;
-    uint32_t off16 = 0u;
-    uint2* pbnd = grp_bnd;
-    bool done = false;
-    // thread 0 of a group: boundary entries of the next two columns, and the
-    // next pair (claimed one pair ahead)
-    uint2 bq0 = make_uint2(Z, Z), bq1 = bq0;
-    Pair2 ninfo{0u, 0u};
-    int my_q = 0;           // stacked: this thread's query in the current pass
-    bool my_first = false;  // stacked: that query starts at this thread's first row
-
-#define SWB_START_PASS()                                                   \
-    {                                                                      \
-        s = 0;                                                             \
-        if (STACKED) {                                                     \
-            const int rb = a.rb_map[pass * T + t];                         \
-            my_first = (rb & kFirstBit) != 0;                              \
-            my_q = (rb < 0) ? -1 : (rb & (kFirstBit - 1));                 \
-            S = Z;                                                         \
-        }                                                                  \
-        nsteps = ncols + 2 * T - 1;                                        \
-        _Pragma("unroll") for (int k = 0; k < R; ++k) {                    \
-            H[k] = Z;                                                      \
-            E[k] = Z;                                                      \
-        }                                                                  \
-        out_h = Z;                                                         \
-        out_f = Z;                                                         \
-        prev_h = Z;                                                        \
-        mid_h = Z;                                                         \
-        mid_f = Z;                                                         \
-        d_bot = kPadPair;                                                  \
-        col = reinterpret_cast<const unsigned short*>(a.db) + (size_t)off16 * 8; \
-        d_cur = (t == 0 && ncols > 0) ? (uint32_t)__ldg(col) : kPadPair;  \
-        if (t == 0) {                                                      \
-            if (pass > 0) {                                                \
-                const uint2* pb = pbnd + ((pass - 1) & 1);                 \
-                bq0 = pb[0];                                               \
-                if (ncols > 1) bq1 = pb[2];                                \
-            }                                                              \
-        }                                                                  \
-    }
-#define SWB_TAKE_PAIR(v)                                                   \
-    {                                                                      \
-        if ((v) >= pair_count) {                                           \
-            done = true;                                                   \
-            ncols = 0;                                                     \
-            nsteps = 0;                                                    \
-        } else {                                                           \
-            pair = (v);                                                    \
-            pass = 0;                                                      \
-            S = Z;                                                         \
-            pbnd = a.bnd_group ? grp_bnd : a.bnd + (size_t)off16 * 16;     \
-            if (t == 0) next = atomicAdd(a.counter, 1);                    \
-            SWB_START_PASS()                                               \
-        }                                                                  \
-    }
-
-    {
-        int v = 0;
-        if (t == 0) v = atomicAdd(a.counter, 1);
-        v = __shfl_sync(gmask, v, 0, T);
-        if (v < pair_count) {
-            const Pair2 pr = a.pairs[a.pair_begin + v];
-            off16 = pr.off16;
-            ncols = (int)pr.ncols;
-        }
-        SWB_TAKE_PAIR(v)
-    }
-
-    while (!__all_sync(FULL, done)) {
-        // thread t-1's bottom half handed down the last-row H and F of the
-        // column it processed in the previous step; every thread loads its
-        // own column's residue pair one step ahead
-        uint32_t h_in = __shfl_up_sync(FULL, out_h, 1, T);
-        uint32_t f_in = __shfl_up_sync(FULL, out_f, 1, T);
-        const uint32_t d_in = d_cur;
-        {
-            const int c1 = s + 1 - 2 * t;     // this thread's top column next step
-            d_cur = (c1 >= 0 && c1 < ncols) ? (uint32_t)__ldg(col + c1) : kPadPair;
-        }
-        if (t == 0) {
-            h_in = Z;
-            f_in = Z;
-            if (s < ncols) {
-                if (pass > 0) {
-                    h_in = bq0.x;
-                    f_in = bq0.y;
-                    bq0 = bq1;
-                    if (s + 2 < ncols) bq1 = pbnd[2 * (s + 2) + ((pass - 1) & 1)];
-                }
-                // the next pair's table entry, once its claim has returned
-                if (pass == 0 && s == (ncols < 9 ? ncols - 1 : 8) && next < pair_count)
-                    ninfo = a.pairs[a.pair_begin + next];
-            }
-        }
-        if (STACKED && my_first) {   // a query starts here: nothing flows in from above
-            h_in = Z;
-            f_in = Z;
-        }
-        const int ct = s - 2 * t;            // top half's column
-        const bool top_valid = ct >= 0 && ct < ncols;
-        const bool bot_valid = ct >= 1 && ct <= ncols;
-        if (!done && (ct >= 0 && ct <= ncols)) {
-            // a half outside the pass's columns runs on zero-score residues:
-            // like a trailing padding column it cannot raise any score
-            const uint32_t wt = top_valid ? d_in : kPadPair;
-            const uint32_t wb = bot_valid ? d_bot : kPadPair;
-            const uint2* prof_p = prof + (pass * NJ) * JSTRIDE + slot;
-            const uint2* t0 = prof_p + (int)(wt & 0xffu) * SLOTS;
-            const uint2* t1 = prof_p + (int)((wt >> 8) & 0xffu) * SLOTS;
-            const uint2* b0 = prof_p + (int)(wb & 0xffu) * SLOTS;
-            const uint2* b1 = prof_p + (int)((wb >> 8) & 0xffu) * SLOTS;
-            const uint32_t bot_diag = mid_h;
-            uint32_t f_top = f_in, f_bot = mid_f;
-            mid_h = H[HALF - 1];     // the top's last row one column back
-            reverse_sweep<R, 0, HALF>(H, E, t0, t1, JSTRIDE, prev_h);
-            reverse_sweep<R, HALF, R>(H, E, b0, b1, JSTRIDE, bot_diag);
-#pragma unroll
-            for (int i = 0; i < HALF; ++i) {
-                forward_cell(H[i], E[i], f_top, K);
-                forward_cell(H[HALF + i], E[HALF + i], f_bot, K);
-                if (i & 1) S = __vimax3_s16x2(S, H[i - 1], H[i]);
-                if (i & 1) S = __vimax3_s16x2(S, H[HALF + i - 1], H[HALF + i]);
-                if (!(i & 1) && i == HALF - 1) S = __vimax3_s16x2(S, H[i], H[HALF + i]);
-            }
-            mid_f = f_top;
-            if (bot_valid) {
-                out_h = H[R - 1];
-                out_f = f_bot;
-                if (t == T - 1 && pass + 1 < P)
-                    pbnd[2 * (ct - 1) + (pass & 1)] = make_uint2(out_h, out_f);
-            }
-        }
-        prev_h = h_in;
-        d_bot = d_in;
-        ++s;
-        if (!done && s == nsteps) {  // uniform within the group
-            __syncwarp(gmask);
-            if (STACKED) {
-                // segmented max over the threads of each query of this pass;
-                // the first thread of a segment adds it to the query's score
-#pragma unroll
-                for (int o = 1; o < T; o <<= 1) {
-                    const uint32_t v = __shfl_down_sync(gmask, S, o, T);
-                    const int qo = __shfl_down_sync(gmask, my_q, o, T);
-                    if (t + o < T && qo == my_q) S = __vimax3_s16x2(S, v, Z);
-                }
-                if (my_q >= 0 && (my_first || t == 0)) {
-                    const int gp = a.pair_ids ? (int)a.pair_ids[a.pair_begin + pair]
-                                              : a.pair_begin + pair;
-                    const int pos = 2 * gp;
-                    const int s0 = lo16(S), s1 = hi16(S);
-                    const int qb = my_q * a.n_records;
-                    atomicMax(a.scores + qb + pos, s0 - bias);
-                    if (s0 >= a.ovf_thresh) {
-                        const int j = atomicAdd(a.ovf_count, 1);
-                        if (j < a.ovf_cap) a.ovf_list[j] = qb + pos;
-                    }
-                    if (pos + 1 < a.n_records) {
-                        atomicMax(a.scores + qb + pos + 1, s1 - bias);
-                        if (s1 >= a.ovf_thresh) {
-                            const int j = atomicAdd(a.ovf_count, 1);
-                            if (j < a.ovf_cap) a.ovf_list[j] = qb + pos + 1;
-                        }
-                    }
-                }
-            }
-            if (pass + 1 < P) {
-                ++pass;
-                SWB_START_PASS()
-            } else if (STACKED) {
-                const int v = __shfl_sync(gmask, next, 0, T);
-                off16 = __shfl_sync(gmask, ninfo.off16, 0, T);
-                ncols = (int)__shfl_sync(gmask, ninfo.ncols, 0, T);
-                SWB_TAKE_PAIR(v)
-            } else {
-#pragma unroll
-                for (int o = T / 2; o > 0; o >>= 1)
-                    S = __vimax3_s16x2(S, __shfl_xor_sync(gmask, S, o, T), Z);
-                if (t == 0) {
-                    const int pos = 2 * (a.pair_begin + pair);
-                    const int s0 = lo16(S), s1 = hi16(S);
-                    a.scores[pos] = s0 - bias;
-                    if (s0 >= a.ovf_thresh) {
-                        const int j = atomicAdd(a.ovf_count, 1);
-                        if (j < a.ovf_cap) a.ovf_list[j] = a.ovf_base + pos;
-                    }
-                    if (pos + 1 < a.n_records) {
-                        a.scores[pos + 1] = s1 - bias;
-                        if (s1 >= a.ovf_thresh) {
-                            const int j = atomicAdd(a.ovf_count, 1);
-                            if (j < a.ovf_cap) a.ovf_list[j] = a.ovf_base + pos + 1;
-                        }
-                    }
-                }
-                const int v = __shfl_sync(gmask, next, 0, T);
-                off16 = __shfl_sync(gmask, ninfo.off16, 0, T);
-                ncols = (int)__shfl_sync(gmask, ninfo.ncols, 0, T);
-                SWB_TAKE_PAIR(v)
-            }
-        }
-    }
-#undef SWB_TAKE_PAIR
-#undef SWB_START_PASS
-}
-
-// Streaming group loop of the plain search.  run_pairs drains the group's
-// wavefront at the end of every pass (2T-1 steps in which part of the group
-// idles), which costs 9 % of the steps at T = 16 on a DB of ~350-residue
-// records and 18 % at T = 32.  Here each thread moves on to the group's next
-// segment (the next pass of the pair, or the next pair) as soon as its own
-// columns of the current one are done, so the wavefront fills only once per
-// launch.  Thread t's top half is on column c of a segment at group step
-// G + c + 2t and its bottom half one column behind, so for one step after a
-// switch the two halves work on different segments: the bottom keeps the
-// profile base and boundary-row view the top had a step earlier.
+// scores them against the query (or query stack) whose profile is in prof;
+// returns when the range is exhausted (warp-wide).
+//
+// The groups stream: each thread moves on to the group's next segment (the
+// next pass of the pair, or the next pair) as soon as its own columns of the
+// current one are done, so the wavefront fills once per range instead of
+// draining for 2T-1 steps at the end of every pass (9 % of the steps at
+// T = 16 on a DB of ~350-residue records, 18 % at T = 32).  Thread t's top
+// half is on column c of a segment at group step G + c + 2t and its bottom
+// half one column behind, so for one step after a switch the two halves work
+// on different segments: the bottom keeps the profile base and boundary-row
+// view the top had a step earlier.
 //   * The pair descriptor (index, stream offset, columns) goes from thread t-1
 //     to thread t by shuffle at t's switch, 2 steps after t-1's.
-//   * A thread's pair maximum is complete one step after its top leaves the
-//     pair's last pass; it travels down the group in a third shuffle (each
-//     thread adds its own), and thread T-1 writes the pair's scores.
+//   * A thread's maximum over a finished pair (plain) or pass (stacked) is
+//     complete one step after its top leaves it; it travels down the group in
+//     a third shuffle, each thread adding its own.  Plain: thread T-1 writes
+//     the pair's scores.  Stacked (several queries share the rows of a pass,
+//     aligned to threads): the chain restarts at a thread whose rows begin a
+//     query, and the last thread of each query's rows adds the query's
+//     maximum with atomicMax (a query longer than a pass is merged over its
+//     passes the same way).
 //   * Thread 0 of pass p+1 reads boundary column j at step G' + j - 2 while
 //     thread T-1 of pass p wrote it at step G + 2T - 1 + j, so a segment that
 //     a later pass depends on lasts at least 2T + 2 steps (padding columns of
 //     zero-score residues, which cannot raise a score); every other segment
 //     lasts at least 3 steps, which keeps the descriptor and maximum hand-offs
 //     one segment apart.
-template <int T, int R>
+template <int T, int R, bool STACKED>
 __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) {
     static_assert(R % 2 == 0 && R >= 4, "R");
-    constexpr int NJ = (R + 7) / 8;
+    constexpr int NJ = (R + 7) / 8;    // 8-row profile chunks per thread (last one partial)
     constexpr int HALF = R / 2;
     constexpr int SLOTS = GroupShape<T>::SLOTS;
     constexpr int JSTRIDE = kCodes * SLOTS;
@@ -466,11 +235,15 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
     K.bias2 = a.bias2;
     K.neg_q2 = 0u - a.bias2;
     K.neg_e2 = a.neg_e;
-    const uint32_t Z = a.bias2;
+    const uint32_t Z = a.bias2;        // biased zero of both lanes
     const int bias = (int)(a.bias2 & 0xffffu);
     const int pair_count = a.pair_count;
     const int dep_steps = 2 * T + 2;
+    uint2* const grp_bnd =
+        a.bnd + (size_t)((blockIdx.x * blockDim.x + threadIdx.x) / T) * a.bnd_group;
 
+    // rows [0, HALF): top half, on column c; rows [HALF, R): bottom half, on
+    // column c - 1 (c = the top's column in its segment)
     uint32_t H[R], E[R];
 #pragma unroll
     for (int k = 0; k < R; ++k) {
@@ -487,13 +260,17 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
     const uint2* prof_t = prof + slot;
     uint2* wrow = a.bnd;       // boundary row this pass writes (thread T-1) ...
     int wlim = 0;              // ... for columns below this (0: last pass)
+    // stacked: this thread's query in the top's pass (-1: padding), whether the
+    // query starts at its first row, whether its last row ends the query's rows
+    int my_q = 0;
+    bool my_first = false, my_last = false;
     // the bottom half's view: the top's of the previous step
     const uint2* prof_b = prof_t;
     uint2* b_wrow = wrow;
     int b_wlim = 0, b_col = -1;
-    // a pair whose maximum is being finished
-    int fpair = 0;
-    bool fpend = false, fin = false;
+    // a segment whose maximum is being finished
+    int fpair = 0, f_q = 0;
+    bool fpend = false, f_first = false, f_last = false, fin = false;
     // thread 0: the next pair (claimed one pair ahead) and the boundary row
     // read by passes after the first (two columns prefetched)
     int next = 0;
@@ -503,14 +280,21 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
 
 #define SWS_SET_SEG()                                                          \
     {                                                                          \
-        nst = ncols > ((pass + 1 < P) ? dep_steps : 3) ? ncols                 \
-                                                       : ((pass + 1 < P) ? dep_steps : 3); \
+        const int lo = (pass + 1 < P) ? dep_steps : 3;                         \
+        nst = ncols > lo ? ncols : lo;                                         \
         col = reinterpret_cast<const unsigned short*>(a.db) + (size_t)off16 * 8; \
-        uint2* const pb = a.bnd + (size_t)off16 * 16;                          \
+        uint2* const pb = a.bnd_group ? grp_bnd : a.bnd + (size_t)off16 * 16;  \
         wrow = pb + (pass & 1);                                                \
         wlim = (pass + 1 < P) ? ncols : 0;                                     \
         rrow = pb + ((pass - 1) & 1);                                          \
         prof_t = prof + pass * PSTRIDE + slot;                                 \
+        if (STACKED) {                                                         \
+            const int rb = a.rb_map[pass * T + t];                             \
+            const int rn = (t + 1 < T) ? a.rb_map[pass * T + t + 1] : -1;      \
+            my_first = (rb & kFirstBit) != 0;                                  \
+            my_q = (rb < 0) ? -1 : (rb & (kFirstBit - 1));                     \
+            my_last = rn < 0 || (rn & kFirstBit) != 0;                         \
+        }                                                                      \
     }
 
     {
@@ -533,6 +317,8 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
 
     while (!__all_sync(FULL, fin)) {
         if (P > 1) __syncwarp();      // orders the boundary row's stores and loads
+        // thread t-1's bottom half handed down the last-row H and F of the
+        // column it processed in the previous step
         uint32_t h_in = __shfl_up_sync(FULL, out_h, 1, T);
         uint32_t f_in = __shfl_up_sync(FULL, out_f, 1, T);
         const uint32_t acc_in = __shfl_up_sync(FULL, acc_out, 1, T);
@@ -554,14 +340,20 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
             if (pass == 0 && c == (nst < 9 ? nst - 1 : 8) && next < pair_count)
                 ninfo = a.pairs[a.pair_begin + next];
         }
+        if (STACKED && my_first) {   // a query starts here: nothing flows in from above
+            h_in = Z;
+            f_in = Z;
+        }
         if (!fin && c >= 0) {
+            // a column past the segment's end runs on zero-score residues:
+            // like a trailing padding column it cannot raise any score
             const uint2* t0 = prof_t + (int)(d_in & 0xffu) * SLOTS;
             const uint2* t1 = prof_t + (int)((d_in >> 8) & 0xffu) * SLOTS;
             const uint2* b0 = prof_b + (int)(d_bot & 0xffu) * SLOTS;
             const uint2* b1 = prof_b + (int)((d_bot >> 8) & 0xffu) * SLOTS;
             const uint32_t bot_diag = mid_h;
             uint32_t f_top = f_in, f_bot = mid_f;
-            mid_h = H[HALF - 1];
+            mid_h = H[HALF - 1];     // the top's last row one column back
             reverse_sweep<R, 0, HALF>(H, E, t0, t1, JSTRIDE, prev_h);
             reverse_sweep<R, HALF, R>(H, E, b0, b1, JSTRIDE, bot_diag);
 #pragma unroll
@@ -588,29 +380,53 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
         b_wlim = wlim;
         b_col = c;
         if (fpend) {
-            // the bottom has just done the finished pair's last column: this
-            // thread's maximum joins the group's, thread T-1 holds the result
+            // the bottom has just done the finished segment's last column:
+            // this thread's maximum joins the chain down the group
             fpend = false;
             uint32_t m = __vimax3_s16x2(S_pend, S_bot, Z);
-            if (t > 0) m = __vimax3_s16x2(m, acc_in, Z);
-            acc_out = m;
-            S_bot = Z;
-            if (t == T - 1) {
-                const int pos = 2 * (a.pair_begin + fpair);
-                const int s0 = lo16(m), s1 = hi16(m);
-                a.scores[pos] = s0 - bias;
-                if (s0 >= a.ovf_thresh) {
-                    const int j = atomicAdd(a.ovf_count, 1);
-                    if (j < a.ovf_cap) a.ovf_list[j] = a.ovf_base + pos;
-                }
-                if (pos + 1 < a.n_records) {
-                    a.scores[pos + 1] = s1 - bias;
-                    if (s1 >= a.ovf_thresh) {
+            if (STACKED) {
+                if (t > 0 && !f_first) m = __vimax3_s16x2(m, acc_in, Z);
+                acc_out = m;
+                if (f_q >= 0 && f_last) {
+                    const int gp = a.pair_ids ? (int)a.pair_ids[a.pair_begin + fpair]
+                                              : a.pair_begin + fpair;
+                    const int pos = 2 * gp;
+                    const int s0 = lo16(m), s1 = hi16(m);
+                    const int qb = f_q * a.n_records;
+                    atomicMax(a.scores + qb + pos, s0 - bias);
+                    if (s0 >= a.ovf_thresh) {
                         const int j = atomicAdd(a.ovf_count, 1);
-                        if (j < a.ovf_cap) a.ovf_list[j] = a.ovf_base + pos + 1;
+                        if (j < a.ovf_cap) a.ovf_list[j] = qb + pos;
+                    }
+                    if (pos + 1 < a.n_records) {
+                        atomicMax(a.scores + qb + pos + 1, s1 - bias);
+                        if (s1 >= a.ovf_thresh) {
+                            const int j = atomicAdd(a.ovf_count, 1);
+                            if (j < a.ovf_cap) a.ovf_list[j] = qb + pos + 1;
+                        }
+                    }
+                }
+            } else {
+                if (t > 0) m = __vimax3_s16x2(m, acc_in, Z);
+                acc_out = m;
+                if (t == T - 1) {
+                    const int pos = 2 * (a.pair_begin + fpair);
+                    const int s0 = lo16(m), s1 = hi16(m);
+                    a.scores[pos] = s0 - bias;
+                    if (s0 >= a.ovf_thresh) {
+                        const int j = atomicAdd(a.ovf_count, 1);
+                        if (j < a.ovf_cap) a.ovf_list[j] = a.ovf_base + pos;
+                    }
+                    if (pos + 1 < a.n_records) {
+                        a.scores[pos + 1] = s1 - bias;
+                        if (s1 >= a.ovf_thresh) {
+                            const int j = atomicAdd(a.ovf_count, 1);
+                            if (j < a.ovf_cap) a.ovf_list[j] = a.ovf_base + pos + 1;
+                        }
                     }
                 }
             }
+            S_bot = Z;
             if (pair >= pair_count) fin = true;
         }
         if (c == 0) {   // the bottom starts this segment's column 0 next step
@@ -627,13 +443,19 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
             const uint32_t up_off = __shfl_up_sync(FULL, off16, 1, T);
             const int up_ncols = __shfl_up_sync(FULL, ncols, 1, T);
             if (adv) {
-                if (pass + 1 < P) {
-                    ++pass;
-                } else {
+                const bool last_pass = pass + 1 >= P;
+                if (STACKED || last_pass) {   // the maximum being finished
                     S_pend = S_top;
                     S_top = Z;
                     fpair = pair;
+                    f_q = my_q;
+                    f_first = my_first;
+                    f_last = my_last;
                     fpend = true;
+                }
+                if (!last_pass) {
+                    ++pass;
+                } else {
                     pass = 0;
                     if (t == 0) {
                         pair = next;
@@ -694,7 +516,7 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
     r.ovf_cap = a.n_records + 1;
     r.pair_ids = nullptr;
     r.rb_map = nullptr;
-    run_stream<T, R>(r, prof);
+    run_stream<T, R, false>(r, prof);
 }
 
 // Batched search: one persistent launch over a list of query stacks (each
@@ -733,7 +555,7 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_batch(const BatchArgs a) {
         r.ovf_cap = a.ovf_cap;
         r.pair_ids = a.pair_ids;
         r.rb_map = a.rb_map + a.rb_off[i];
-        run_pairs<T, R, true>(r, prof);
+        run_stream<T, R, true>(r, prof);
     }
 }
 
