@@ -264,7 +264,8 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
     // query starts at its first row, whether its last row ends the query's rows
     int my_q = 0;
     bool my_first = false, my_last = false;
-    // the bottom half's view: the top's of the previous step
+    // the bottom half's view: the top's of the previous step (the profile base
+    // and boundary row change only when the bottom reaches a segment's column 0)
     const uint2* prof_b = prof_t;
     uint2* b_wrow = wrow;
     int b_wlim = 0, b_col = -1;
@@ -273,7 +274,7 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
     bool fpend = false, f_first = false, f_last = false, fin = false;
     // thread 0: the next pair (claimed one pair ahead) and the boundary row
     // read by passes after the first (two columns prefetched)
-    int next = 0;
+    int next = 0, nload = -1;   // nload: the step of the first pass that loads its entry
     Pair2 ninfo{0u, 0u};
     uint2 bq0 = make_uint2(Z, Z), bq1 = bq0;
     const uint2* rrow = a.bnd;
@@ -288,6 +289,7 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
         wlim = (pass + 1 < P) ? ncols : 0;                                     \
         rrow = pb + ((pass - 1) & 1);                                          \
         prof_t = prof + pass * PSTRIDE + slot;                                 \
+        nload = (pass == 0) ? (nst < 9 ? nst - 1 : 8) : -1;                    \
         if (STACKED) {                                                         \
             const int rb = a.rb_map[pass * T + t];                             \
             const int rn = (t + 1 < T) ? a.rb_map[pass * T + t + 1] : -1;      \
@@ -311,6 +313,9 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
             fin = true;
         }
         SWS_SET_SEG()
+        prof_b = prof_t;
+        b_wrow = wrow;
+        b_wlim = wlim;
         c = -2 * t;
         d_cur = (t == 0 && ncols > 0) ? (uint32_t)__ldg(col) : kPadPair;
     }
@@ -337,8 +342,7 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
                 if (c + 2 < ncols) bq1 = rrow[2 * (c + 2)];
             }
             // the next pair's table entry, once its claim has returned
-            if (pass == 0 && c == (nst < 9 ? nst - 1 : 8) && next < pair_count)
-                ninfo = a.pairs[a.pair_begin + next];
+            if (c == nload && next < pair_count) ninfo = a.pairs[a.pair_begin + next];
         }
         if (STACKED && my_first) {   // a query starts here: nothing flows in from above
             h_in = Z;
@@ -375,70 +379,73 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
         }
         prev_h = h_in;
         d_bot = d_in;
-        prof_b = prof_t;
-        b_wrow = wrow;
-        b_wlim = wlim;
         b_col = c;
-        if (fpend) {
-            // the bottom has just done the finished segment's last column:
-            // this thread's maximum joins the chain down the group
-            fpend = false;
-            uint32_t m = __vimax3_s16x2(S_pend, S_bot, Z);
-            if (STACKED) {
-                if (t > 0 && !f_first) m = __vimax3_s16x2(m, acc_in, Z);
-                acc_out = m;
-                if (f_q >= 0 && f_last) {
-                    const int gp = a.pair_ids ? (int)a.pair_ids[a.pair_begin + fpair]
-                                              : a.pair_begin + fpair;
-                    const int pos = 2 * gp;
-                    const int s0 = lo16(m), s1 = hi16(m);
-                    const int qb = f_q * a.n_records;
-                    atomicMax(a.scores + qb + pos, s0 - bias);
-                    if (s0 >= a.ovf_thresh) {
-                        const int j = atomicAdd(a.ovf_count, 1);
-                        if (j < a.ovf_cap) a.ovf_list[j] = qb + pos;
-                    }
-                    if (pos + 1 < a.n_records) {
-                        atomicMax(a.scores + qb + pos + 1, s1 - bias);
-                        if (s1 >= a.ovf_thresh) {
+        // segment events, one warp vote per step: a finished maximum, the
+        // bottom entering a segment, the top leaving one
+        const bool ev = fpend || c == 0 || (!fin && c == nst - 1);
+        if (__any_sync(FULL, ev)) {
+            if (fpend) {
+                // the bottom has just done the finished segment's last column:
+                // this thread's maximum joins the chain down the group
+                fpend = false;
+                uint32_t m = __vimax3_s16x2(S_pend, S_bot, Z);
+                if (STACKED) {
+                    if (t > 0 && !f_first) m = __vimax3_s16x2(m, acc_in, Z);
+                    acc_out = m;
+                    if (f_q >= 0 && f_last) {
+                        const int gp = a.pair_ids ? (int)a.pair_ids[a.pair_begin + fpair]
+                                                  : a.pair_begin + fpair;
+                        const int pos = 2 * gp;
+                        const int s0 = lo16(m), s1 = hi16(m);
+                        const int qb = f_q * a.n_records;
+                        atomicMax(a.scores + qb + pos, s0 - bias);
+                        if (s0 >= a.ovf_thresh) {
                             const int j = atomicAdd(a.ovf_count, 1);
-                            if (j < a.ovf_cap) a.ovf_list[j] = qb + pos + 1;
+                            if (j < a.ovf_cap) a.ovf_list[j] = qb + pos;
+                        }
+                        if (pos + 1 < a.n_records) {
+                            atomicMax(a.scores + qb + pos + 1, s1 - bias);
+                            if (s1 >= a.ovf_thresh) {
+                                const int j = atomicAdd(a.ovf_count, 1);
+                                if (j < a.ovf_cap) a.ovf_list[j] = qb + pos + 1;
+                            }
+                        }
+                    }
+                } else {
+                    if (t > 0) m = __vimax3_s16x2(m, acc_in, Z);
+                    acc_out = m;
+                    if (t == T - 1) {
+                        const int pos = 2 * (a.pair_begin + fpair);
+                        const int s0 = lo16(m), s1 = hi16(m);
+                        a.scores[pos] = s0 - bias;
+                        if (s0 >= a.ovf_thresh) {
+                            const int j = atomicAdd(a.ovf_count, 1);
+                            if (j < a.ovf_cap) a.ovf_list[j] = a.ovf_base + pos;
+                        }
+                        if (pos + 1 < a.n_records) {
+                            a.scores[pos + 1] = s1 - bias;
+                            if (s1 >= a.ovf_thresh) {
+                                const int j = atomicAdd(a.ovf_count, 1);
+                                if (j < a.ovf_cap) a.ovf_list[j] = a.ovf_base + pos + 1;
+                            }
                         }
                     }
                 }
-            } else {
-                if (t > 0) m = __vimax3_s16x2(m, acc_in, Z);
-                acc_out = m;
-                if (t == T - 1) {
-                    const int pos = 2 * (a.pair_begin + fpair);
-                    const int s0 = lo16(m), s1 = hi16(m);
-                    a.scores[pos] = s0 - bias;
-                    if (s0 >= a.ovf_thresh) {
-                        const int j = atomicAdd(a.ovf_count, 1);
-                        if (j < a.ovf_cap) a.ovf_list[j] = a.ovf_base + pos;
-                    }
-                    if (pos + 1 < a.n_records) {
-                        a.scores[pos + 1] = s1 - bias;
-                        if (s1 >= a.ovf_thresh) {
-                            const int j = atomicAdd(a.ovf_count, 1);
-                            if (j < a.ovf_cap) a.ovf_list[j] = a.ovf_base + pos + 1;
-                        }
-                    }
-                }
+                S_bot = Z;
+                if (pair >= pair_count) fin = true;
             }
-            S_bot = Z;
-            if (pair >= pair_count) fin = true;
-        }
-        if (c == 0) {   // the bottom starts this segment's column 0 next step
+            if (c == 0) {   // the bottom starts this segment's column 0 next step
 #pragma unroll
-            for (int k = HALF; k < R; ++k) {
-                H[k] = Z;
-                E[k] = Z;
+                for (int k = HALF; k < R; ++k) {
+                    H[k] = Z;
+                    E[k] = Z;
+                }
+                prof_b = prof_t;
+                b_wrow = wrow;
+                b_wlim = wlim;
             }
-        }
-        // the top leaves its segment: set up the next one
-        const bool adv = !fin && c == nst - 1;
-        if (__any_sync(FULL, adv)) {
+            // the top leaves its segment: set up the next one
+            const bool adv = !fin && c == nst - 1;
             const int up_pair = __shfl_up_sync(FULL, pair, 1, T);
             const uint32_t up_off = __shfl_up_sync(FULL, off16, 1, T);
             const int up_ncols = __shfl_up_sync(FULL, ncols, 1, T);
