@@ -244,8 +244,11 @@ sw_status sw_search_device(struct sw_ctx *ctx, const uint8_t *d_query,
 sw_status sw_set_kernel_config(struct sw_ctx *ctx, const sw_kernel_config *cfg);
 
 /* Shape table from the autotuner: for a query of qlen residues the first
- * entry (in the given order, sorted by max_qlen) with qlen <= max_qlen is used.
- * n = 0 clears the table (the built-in cost model is used again). */
+ * entry (in the given order, sorted by max_qlen) with qlen <= max_qlen is used
+ * when its shapes fit that length (else the cost model chooses).  A new
+ * context starts with the table measured on B200 that is compiled into the
+ * library (swhybrid_b200/tuned/b200.json); this call replaces it, and n = 0
+ * clears it (the cost model alone chooses). */
 typedef struct sw_tuning_entry {
     uint32_t max_qlen;
     sw_kernel_config cfg;

@@ -16,6 +16,7 @@
 #include <chrono>
 #include <cstdio>
 #include <cstring>
+#include <iterator>
 #include <mutex>
 #include <numeric>
 #include <string>
@@ -28,6 +29,7 @@
 #include "sw_device.cuh"
 #include "sw_engine.h"
 #include "sw_long.h"
+#include "sw_tuned_default.h"
 #include "sw_registry.h"
 
 namespace swb {
@@ -185,6 +187,7 @@ extern "C" sw_status sw_ctx_create(int device, const sw_params* params, sw_ctx**
     if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess)
         return fail(SW_ERR_CUDA);
     ctx->stream = ctx->own_stream;
+    ctx->tuning.assign(std::begin(kDefaultTuning), std::end(kDefaultTuning));
     if (cudaStreamCreateWithFlags(&ctx->side_stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming) != cudaSuccess ||
         cudaEventCreateWithFlags(&ctx->join_ev, cudaEventDisableTiming) != cudaSuccess)
@@ -251,6 +254,7 @@ static void free_db(sw_ctx* ctx) {
     ctx->n_records = 0;
     ctx->n_pairs = 0;
     ctx->pair_ncols.clear();
+    ctx->pair_prefix.clear();
     ctx->db_loaded = false;
 }
 
@@ -378,10 +382,12 @@ sw_status swb::db_load(sw_ctx* ctx, const uint8_t* residues, const uint64_t* off
     ctx->max_len = maxlen;
     ctx->units = units;
     ctx->pair_ncols.resize(nonempty);
+    ctx->pair_prefix.assign(nonempty + 1, 0u);
     ctx->pair_cols_total = 0;
     for (uint64_t p = 0; p < nonempty; ++p) {
         ctx->pair_ncols[p] = pairs[p].ncols;
         ctx->pair_cols_total += pairs[p].ncols;
+        ctx->pair_prefix[p + 1] = ctx->pair_cols_total;
     }
     auto nomem = [&](const char* what) {
         free_db(ctx);
@@ -441,19 +447,34 @@ int shape_occupancy(sw_ctx* ctx, const WfKernel& k, int qlen) {
     return nb;
 }
 
-// Modelled cost of running pairs [b, e) with a shape: DPX-pipe instructions
-// (about 6.75 per cell pair plus ~20 per thread step) spread over the warps
-// the SM can keep resident, plus the wavefront fill of T-1 steps per pass.
+// Sum over the pairs [b, e) of max(ncols, m): the column steps of one pass
+// whose segments last at least m steps.  Pairs are sorted by ncols
+// descending, so the pairs below m are a suffix of the range.
+double cols_at_least(const sw_ctx* ctx, int64_t b, int64_t e, uint32_t m) {
+    const auto first = ctx->pair_ncols.begin();
+    const int64_t i = std::partition_point(first + b, first + e,
+                                           [m](uint32_t n) { return n >= m; }) - first;
+    return (double)(ctx->pair_prefix[i] - ctx->pair_prefix[b]) + (double)m * (double)(e - i);
+}
+
+// Modelled cost of running pairs [b, e) with a shape, for contexts without a
+// shape table entry that fits: thread steps x (R + 12.9) plus 25 per pass
+// column and group, over an efficiency by group width (several groups in a
+// warp diverge at their pair switches) and by resident warps.  The constants
+// were fitted to the sweep of every compiled shape at 20 query lengths on a
+// B200 (570,200 records); the model's pick is within 0.93 of the best shape
+// on average there.  Columns per pass are counted as the streaming loop runs
+// them: at least 2T + 2 steps for a pass a later pass depends on, 3 otherwise.
 double shape_cost(sw_ctx* ctx, const WfKernel& k, int qlen, int64_t b, int64_t e) {
     const int occ = shape_occupancy(ctx, k, qlen);
     if (occ == 0 || e <= b) return occ == 0 ? 1e300 : 0.0;
     const double P = (qlen + k.T * k.R - 1) / (k.T * k.R);
-    double cols = 0;
-    for (int64_t p = b; p < e; ++p) cols += ctx->pair_ncols[p] + k.T - 1;
-    const double instr = P * cols * k.T * (6.75 * k.R + 20.0);
+    const double cols = (P - 1) * cols_at_least(ctx, b, e, 2 * k.T + 2) + cols_at_least(ctx, b, e, 3);
+    const double work = cols * (k.T * (k.R + 12.9) + 25.1);
+    const double g_width = k.T >= 32 ? 1.0 : k.T >= 16 ? 0.854 : k.T >= 8 ? 0.687 : 0.663;
     const double warps = (double)occ * k.block / 32.0;
-    const double eff = std::min(1.0, warps / 12.0);
-    return instr / eff;
+    const double g_warps = warps < 12 ? 0.912 : warps < 20 ? 1.0 : 1.09;
+    return work / (g_width * g_warps);
 }
 
 sw_kernel_config choose_config(sw_ctx* ctx, int qlen) {
@@ -468,7 +489,6 @@ sw_kernel_config choose_config(sw_ctx* ctx, int qlen) {
     }
     int n = 0;
     const WfKernel* ks = wf_kernels(&n);
-    // evaluate on a sample of pairs to keep this cheap on big DBs
     const int64_t np = ctx->n_pairs;
     double best = 1e301;
     sw_kernel_config cfg{32, 32, 32, 32, 0};

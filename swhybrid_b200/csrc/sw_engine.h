@@ -81,6 +81,7 @@ struct sw_ctx {
     uint64_t db_bytes = 0;
     std::vector<uint32_t> pair_ncols;  // host copy, for shape selection
     uint64_t pair_cols_total = 0;      // sum of pair_ncols
+    std::vector<uint64_t> pair_prefix; // pair_prefix[p] = sum of pair_ncols[0, p)
     std::vector<uint32_t> rec_pos;     // record -> sorted position (host)
     std::vector<uint32_t> rec_len;     // record -> length (host)
     uint4* d_db = nullptr;

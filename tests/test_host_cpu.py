@@ -97,5 +97,8 @@ def test_tuning_table_accounts_for_pass_padding():
     assert [hi for hi, _ in tab] == sorted(hi for hi, _ in tab)
     committed = autotune.load_table()
     assert committed and [hi for hi, _ in committed] == sorted(hi for hi, _ in committed)
+    # the library's built-in table is the committed one
+    from swhybrid_b200 import build
+    assert open(build.DEFAULT_HEADER).read() == build.default_header_text()
     shapes = set(capi.shapes())
     assert all((c[0], c[1]) in shapes and (c[2], c[3]) in shapes for _, c in committed)
