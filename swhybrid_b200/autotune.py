@@ -81,6 +81,17 @@ def rows_used(T: int, R: int, qlen: int) -> int:
     return -(-qlen // (T * R)) * T * R
 
 
+SMEM_OPTIN = 232_448      # B200 shared memory a block may opt in to (bytes)
+CODES = 25                # profile rows per pass chunk (residue codes incl. the zero code)
+
+
+def profile_fits(T: int, R: int, qlen: int) -> bool:
+    """Whether the query profile of a shape fits a block's shared memory (the
+    library's wf_smem_bytes: passes x 8-row chunks x codes x slots x 8 B)."""
+    passes = -(-qlen // (T * R))
+    return passes * ((R + 7) // 8) * CODES * max(T, 16) * 8 <= SMEM_OPTIN
+
+
 def predict_gcups(results, shape: str, qlen: int) -> float | None:
     """GCUPS of a shape at any query length from the sweep: a shape's rate on
     the rows it computes (measured GCUPS x rows computed / qlen) changes slowly
@@ -89,6 +100,8 @@ def predict_gcups(results, shape: str, qlen: int) -> float | None:
     the two measured lengths around qlen; None if the shape was not measured
     at both (its profile did not fit) or qlen is far past the last one."""
     T, R = (int(x) for x in shape.split("x"))
+    if not profile_fits(T, R, qlen):
+        return None
     Ls = sorted(results)
 
     def rate(L):
