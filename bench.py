@@ -20,8 +20,8 @@ cpu_baseline: the reference's own AVX2 kernels (avxCompute + avxCompute16,
         compiled from the reference sources into oracle/_ref) on a bounded
         sample of the same workload, all host threads.
 
---impl reference runs only the reference's CPU kernels (rank 0) on a bounded
-sample per step and prints the same metric.
+--impl reference runs only the reference's CPU kernels (rank 0), one step =
+the whole sweep against the full DB, and prints the same metric.
 
 Multi-GPU (torchrun): every rank holds its own 205 M-residue DB shard (a
 different seed) and runs the same sweep; the work is independent per rank
@@ -62,7 +62,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=list(WORKLOADS), default="full")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0,
+    ap.add_argument("--cpu-seconds", type=float, default=30.0,
                     help="target CPU time of the bounded reference sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--config", type=str, default=None,
@@ -167,7 +167,7 @@ def probe_rates(device: int):
     L = ctypes.CDLL(path)
     L.swprobe_rates.restype = ctypes.c_int
     L.swprobe_rates.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.c_int]
-    out = (ctypes.c_double * 16)()
+    out = (ctypes.c_double * 20)()
     rc = L.swprobe_rates(device, out, 4096)
     if rc != 0:
         raise RuntimeError(f"swprobe_rates failed: {rc}")
@@ -186,33 +186,74 @@ def probe_rates(device: int):
         "hmax2_instr_per_clk_sm": per(out[11], 2),
         "hadd2_instr_per_clk_sm": per(out[12], 2),
         "hmax2_dpx_mix_instr_per_clk_sm": per(out[13], 2),
+        # 8-bit first pass (four records per register): CUDA's byte-SIMD
+        # functions, and the same cell built by hand from 32-bit operations
+        "cell8_intrinsics_gcups": out[14] / 1e9,
+        "cell8_swar_gcups": out[15] / 1e9,
+        # the batched kernel's paired-query cell (no per-row byte unpacking)
+        "cell_pair_mix_gcups": out[16] / 1e9,
         "sms": int(sms), "attr_clock_mhz": mhz,
     }
 
 
 # ---------------------------------------------------------------------------
-def cpu_baseline(db, queries, target_s: float):
-    """The reference's own AVX2 kernels on a bounded sample of the sweep."""
+def _parity_entry(n_checked, n_records, mismatches, top_equal):
+    return {"queries": n_checked, "records": n_records, "mismatches": mismatches,
+            "top10_equal": top_equal}
+
+
+def cpu_baseline(db, queries, target_s: float, gpu=None):
+    """The reference's own AVX2 kernels on a bounded sample of the sweep.
+
+    gpu: optional {"sweep": [(hits, scores) per query], "batched": [(query,
+    hits, scores)]} from the GPU run on the same DB; every record score the
+    reference kernels produce here is compared with it (full-size parity)."""
     import oracle
     from swhybrid_b200 import param
     m = param.blosum62()
     threads = oracle.ref_threads()
     rdb = oracle.RefDB(db.residues, db.offsets)
     cells, secs, used = 0, 0.0, []
+    bad, top_ok, checked = 0, True, 0
     order = list(range(0, len(queries), 4)) + [i for i in range(len(queries)) if i % 4]
     for i in order:
         q = queries[i]
-        _, s, _ = rdb.search(q, m, 10, 2, threads=threads)
+        want, s, _ = rdb.search(q, m, 10, 2, threads=threads)
         cells += len(q) * db.total
         secs += s
         used.append(len(q))
+        if gpu is not None and gpu.get("sweep"):
+            hits, sc = gpu["sweep"][i]
+            bad += int(np.count_nonzero(sc != want))
+            top_ok &= _top_equal(hits, want)
+            checked += 1
         if secs >= target_s:
             break
+    parity = None
+    if gpu is not None:
+        parity = {"sweep": _parity_entry(checked, int(db.n), bad, bool(top_ok))}
+        bb, bt = 0, True
+        for q, hits, sc in gpu.get("batched", []):
+            want, _, _ = rdb.search(q, m, 10, 2, threads=threads)
+            bb += int(np.count_nonzero(sc != want))
+            bt &= _top_equal(hits, want)
+        if gpu.get("batched"):
+            parity["batched"] = _parity_entry(len(gpu["batched"]), int(db.n), bb, bool(bt))
+            parity["batched"]["query_lengths"] = [len(q) for q, _, _ in gpu["batched"]]
+        parity["reference"] = "avxCompute + avxCompute16 (oracle/_ref), every record of the DB"
     rdb.close()
     return {"value": cells / secs / 1e9, "unit": "GCUPS", "cores": threads,
             "kind": "reference",
             "sample": f"reference avxCompute+avxCompute16 on the full {db.n}-record DB, "
-                      f"query lengths {used} ({secs:.1f} s of kernel time)"}, secs
+                      f"query lengths {used} ({secs:.1f} s of kernel time)"}, secs, parity
+
+
+def _top_equal(hits, want_scores, k=10) -> bool:
+    """The GPU hit list equals the top-k of the reference scores under the
+    stated order (score descending, then index ascending)."""
+    import oracle
+    ws, wi = oracle.topk(want_scores, k)
+    return [h[0] for h in hits] == ws.tolist() and [h[1] for h in hits] == wi.tolist()
 
 
 # ---------------------------------------------------------------------------
@@ -226,12 +267,11 @@ def run_reference(args, rank, world):
     m = param.blosum62()
     threads = oracle.ref_threads()
     rdb = oracle.RefDB(db.residues, db.offsets)
-    # bounded sample per step: every fourth query of the sweep
-    sample = queries[::4] if len(queries) > 1 else queries
+    # one step = the whole sweep, as in the GPU arm; warm-up = the shortest query
+    sample = queries
     cells_step = sum(len(q) for q in sample) * db.total
     for _ in range(args.warmup):
-        for q in sample[:1]:
-            rdb.search(q, m, 10, 2, threads=threads)
+        rdb.search(min(sample, key=len), m, 10, 2, threads=threads)
     secs = 0.0
     for _ in range(args.steps):
         for q in sample:
@@ -248,8 +288,8 @@ def run_reference(args, rank, world):
                    "l2": "DB (205 MB) larger than L2"},
         "cpu_baseline": {"value": round(value, 3), "unit": "GCUPS", "cores": threads,
                          "kind": "reference",
-                         "sample": f"every 4th query of the sweep against the full DB, "
-                                   f"{args.steps} steps"},
+                         "sample": f"the whole {len(sample)}-query sweep against the full DB "
+                                   f"per step, {args.steps} steps"},
         "e2e": {"value": round(value, 3), "unit": "GCUPS", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -460,7 +500,7 @@ def run_ours(args, rank, world, local_rank):
                               "first_pass_launches": int(tot.first_pass_launches),
                               "config": list(ctx.kernel_config(len(queries[0])))}), flush=True)
         ctx.close()
-        return None, db, queries
+        return None, db, queries, None
 
     # ---- timed: end to end through sw_search (host buffers) ----
     ctx.set_stream(None)
@@ -480,6 +520,12 @@ def run_ours(args, rank, world, local_rank):
     barrier()
     e2e_s_max = max_over_ranks(e2e_s)
     e2e_value = cells_step * args.steps * world / e2e_s_max / 1e9
+
+    # every record's score for the sweep, checked against the reference's own
+    # kernels by the CPU-baseline leg (untimed)
+    gpu_scores = None
+    if rank == 0 and world == 1 and args.workload == "full" and not args.no_cpu_baseline:
+        gpu_scores = {"sweep": [ctx.search(q, want_scores=True) for q in hq], "batched": []}
 
     # ---- batched: 64 queries, lengths log-uniform 50..5,000, one call ----
     batched = None
@@ -516,6 +562,14 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         plain_ms = max_over_ranks(pev0.elapsed_time(pev1))
         ctx.set_stream(None)
+        if gpu_scores is not None:
+            # the shortest, the longest and two middle queries of the batch
+            bh, bs = ctx.search_batch(bq, want_scores=True)
+            order = np.argsort([len(q) for q in bq], kind="stable")
+            picks = sorted({int(order[0]), int(order[len(bq) // 3]),
+                            int(order[2 * len(bq) // 3]), int(order[-1])})
+            gpu_scores["batched"] = [(bq[i], bh[i], bs[i].copy()) for i in picks]
+            del bs
         batched = {
             "workload": "64 queries, lengths log-uniform 50..5,000 (seeded), full-size DB, "
                         "one sw_search_batch call (CUDA graph replay)",
@@ -617,7 +671,7 @@ def run_ours(args, rank, world, local_rank):
         if stress is not None:
             line["stress"] = stress
     ctx.close()
-    return line, db, queries
+    return line, db, queries, gpu_scores
 
 
 def main():
@@ -634,11 +688,13 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
-    line, db, queries = run_ours(args, rank, world, local_rank)
+    line, db, queries, gpu_scores = run_ours(args, rank, world, local_rank)
     if line is None:
         return 0
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cb, _ = cpu_baseline(db, queries, args.cpu_seconds)
+        cb, _, parity = cpu_baseline(db, queries, args.cpu_seconds, gpu_scores)
+        if parity is not None:
+            line["parity"] = parity
         line["cpu_baseline"] = {k: (round(v, 3) if isinstance(v, float) else v)
                                 for k, v in cb.items()}
     if rank == 0 and line is not None:

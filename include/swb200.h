@@ -443,19 +443,23 @@ sw_status sw_serve_stop(struct sw_ctx *ctx);
 /* ---- scoring without allocation ------------------------------------------ */
 
 /* No counterpart in the reference.  For callers that cannot call cudaMalloc
- * at this point -- a request path that must not allocate after start-up, a
- * plug-in whose host process owns all device memory through its own
- * allocator, work enqueued while a stream is being captured.  Scores every
- * record of a DB that the caller already holds in device memory (codes 0..24
- * back to back, n_records+1 device offsets) against a device query, exactly
- * (int32; min(score, 65535) with SW_FLAG_REFERENCE_CAP), into d_scores
- * (n_records int32, device).  Allocates nothing: its scratch is one static
- * device array of about 16 MiB inside libswb200.so, held by every GPU that
- * loads the library until the process exits.  Limit: records of at most
- * 8192 residues (longer ones give SW_ERR_UNSUPPORTED and score 0).  The
- * first call on a device looks up the array's address, so make it before any
- * stream capture.  Synchronous on cuda_stream (NULL = default stream).  All
- * calls share the array: calls that overlap on the GPU race. */
+ * where they score: a request path that must not allocate once it has
+ * started (an allocation can block on the driver and stall every request
+ * behind it), or a plug-in inside a host process whose device memory is all
+ * reserved by that process's own allocator.  Scores every record of a DB
+ * that the caller already holds in device memory (codes 0..24 back to back,
+ * n_records+1 device offsets) against a device query, exactly (int32;
+ * min(score, 65535) with SW_FLAG_REFERENCE_CAP), into d_scores (n_records
+ * int32, device).  Allocates nothing: its scratch is one static device array
+ * of about 16 MiB inside libswb200.so, held by every GPU that loads the
+ * library until the process exits.  Limits: records of at most 8192
+ * residues (a longer one scores 0 and the call returns SW_ERR_UNSUPPORTED
+ * after scoring the others), at most 2^31 - 1 records and 2^24 query
+ * residues (SW_ERR_UNSUPPORTED, nothing scored).  The first call on a device
+ * looks up the array's device address; make that first call before any
+ * stream capture.  The call waits for its own work on cuda_stream (NULL =
+ * the default stream) before it returns.  All calls share the array and
+ * each starts by clearing its counter: calls that overlap on the GPU race. */
 sw_status sw_score_noalloc(int device, const sw_params *params, const uint8_t *d_query,
                            uint32_t qlen, const uint8_t *d_residues,
                            const uint64_t *d_offsets, uint32_t n_records, int32_t *d_scores,

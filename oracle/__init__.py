@@ -27,10 +27,17 @@ _c_i32 = ctypes.c_int32
 _ptr = ctypes.c_void_p
 
 
+def reference_root() -> str:
+    """The read-only reference source tree: the SWHYBRID_REF environment
+    variable, by default the checkout this container mounts."""
+    return os.environ.get("SWHYBRID_REF", "/root/reference")
+
+
 def build(quiet: bool = True) -> None:
     """Compile the C restatement and, when the reference tree is present,
     the reference kernels."""
-    out = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+    out = subprocess.run(["make", "-C", HERE, f"SWHYBRID_REF={reference_root()}"],
+                         capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
     if not quiet:

@@ -15,6 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libswb200.so")
 
 SW_OK = 0
+SW_ERR_UNSUPPORTED = 6
 STATUS = {
     0: "SW_OK", 1: "SW_ERR_INVALID", 2: "SW_ERR_CUDA", 3: "SW_ERR_NOMEM",
     4: "SW_ERR_STATE", 5: "SW_ERR_FORMAT", 6: "SW_ERR_UNSUPPORTED",

@@ -1,15 +1,15 @@
 // sw_noalloc.cu -- scoring entry point that allocates no memory.
 //
-// Some callers cannot call cudaMalloc: code running on a request path that
-// must never allocate after start-up (latency-bound serving loops), plug-ins
-// living in a host process whose device memory is owned by another allocator
-// that has reserved it, or code that enqueues work while a stream is being
-// captured into a CUDA graph.  sw_score_noalloc serves them: the caller
-// passes device inputs and a device output, and every byte of scratch the
-// kernel needs comes from one file-scope __device__ array that is part of the
-// loaded library image.  That array (256 warps x 8192 columns x 8 bytes plus
-// a 256-byte header, about 16 MiB) is held by every GPU that loads the
-// library until the process exits.
+// Some callers cannot call cudaMalloc where they score: a request path that
+// must never allocate once it has started (an allocation can block on the
+// driver and stall every request queued behind it), or a plug-in living in a
+// host process whose device memory is all reserved by that process's own
+// allocator.  sw_score_noalloc serves them: the caller passes device inputs
+// and a device output, and every byte of scratch the kernel needs comes from
+// one file-scope __device__ array that is part of the loaded library image.
+// That array (256 warps x 8192 columns x 8 bytes plus a 256-byte header,
+// about 16 MiB) is held by every GPU that loads the library until the
+// process exits.
 //
 // The kernel is a variant of the exact 32-bit re-score pass (sw_rescore32,
 // sw_aux.cu): one warp per record, anti-diagonal wavefront over 32 lanes x 16
@@ -17,6 +17,7 @@
 // passes lives in the warp's slice of the static array instead of the DB's
 // boundary buffer.  Records are claimed through a counter that also lives in
 // the static array.
+#include <climits>
 #include <cstdint>
 #include <cstring>
 #include <mutex>
@@ -157,7 +158,7 @@ extern "C" sw_status sw_score_noalloc(int device, const sw_params* params, const
         return SW_ERR_INVALID;
     for (int i = 0; i < 1024; ++i)
         if (params->matrix[i] < -127 || params->matrix[i] > 127) return SW_ERR_INVALID;
-    if (qlen > (1u << 24)) return SW_ERR_UNSUPPORTED;
+    if (qlen > (1u << 24) || n_records > (uint32_t)INT32_MAX) return SW_ERR_UNSUPPORTED;
     int prev = 0;
     if (cudaGetDevice(&prev) != cudaSuccess) return SW_ERR_CUDA;
     if (cudaSetDevice(device) != cudaSuccess) return SW_ERR_NO_DEVICE;
