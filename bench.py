@@ -55,7 +55,7 @@ WORKLOADS = {
 
 
 # ---------------------------------------------------------------------------
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=3)
@@ -75,7 +75,10 @@ def parse():
                     help="skip the overflow / long-record stress measurement")
     ap.add_argument("--kernel-only", action="store_true",
                     help="time the resident path only (no e2e, probe or CPU baseline)")
-    return ap.parse_args()
+    ap.add_argument("--shard", action="store_true",
+                    help="one DB split over the ranks (residue-balanced shards, all-gather "
+                         "of k hits per query): strong scaling of the sharded search")
+    return ap.parse_args(argv)
 
 
 def make_workload(name: str, rank: int):
@@ -674,8 +677,77 @@ def run_ours(args, rank, world, local_rank):
     return line, db, queries, gpu_scores
 
 
-def main():
-    args = parse()
+def run_shard(args, rank, world, local_rank, make_ctx=None, workload=None):
+    """--shard: ONE DB (rank 0's seed on every rank) split into contiguous,
+    residue-balanced record ranges, one per rank (swhybrid_b200/shard.py);
+    every query is searched by all ranks on their shards and the k best hits
+    are merged by one all-gather per query (WorkerPool's split of one DB over
+    its workers, src/WorkerPool.cpp:10-105).  value = cells of the whole DB x
+    the queries / the max-over-ranks time of the steps (strong scaling).
+
+    make_ctx / workload stand in for the device context and the workload in
+    the CPU test of this path (gloo ranks, the oracle as each rank's search).
+    Returns (line or None, the merged hit lists of the last step)."""
+    import torch
+    import torch.distributed as dist
+    from swhybrid_b200 import shard as _shard
+    db, queries = workload if workload is not None else make_workload(args.workload, 0)
+    on_gpu = make_ctx is None
+    if on_gpu:
+        from swhybrid_b200 import autotune, capi
+        torch.cuda.set_device(local_rank)
+        ctx = capi.Context(local_rank, capi.default_params(top_k=10))
+    else:
+        ctx = make_ctx()
+    try:
+        searcher = _shard.ShardedSearch(ctx, db.residues, db.offsets, rank, world)
+        if on_gpu:
+            autotune.apply(ctx)
+        for _ in range(args.warmup):
+            searcher.search(queries[0])
+        dist.barrier()
+        if on_gpu:
+            torch.cuda.synchronize()
+            ev0 = torch.cuda.Event(enable_timing=True)
+            ev1 = torch.cuda.Event(enable_timing=True)
+            ev0.record()
+        t0 = time.perf_counter()
+        merged = []
+        for _ in range(args.steps):
+            merged = [searcher.search(q) for q in queries]
+        if on_gpu:
+            ev1.record()
+            torch.cuda.synchronize()
+            ms = ev0.elapsed_time(ev1)
+        else:
+            ms = (time.perf_counter() - t0) * 1e3
+        t = torch.tensor([ms], dtype=torch.float64,
+                         device=f"cuda:{local_rank}" if on_gpu else "cpu")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+        local_res = int(db.offsets[searcher.end] - db.offsets[searcher.begin])
+        cells = sum(len(q) for q in queries) * db.total * args.steps
+        line = None
+        if rank == 0:
+            line = {
+                "metric": METRIC, "value": round(cells / (ms_max * 1e-3) / 1e9, 3),
+                "unit": "GCUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": round(ms_max / args.steps, 3), "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None, "dtype": "int16x2 (int32 re-score)",
+                "data": "synthetic (seeded; Robinson & Robinson 1991 residue frequencies)",
+                "config": {"workload": WORKLOADS[args.workload] + "; the DB split over the ranks",
+                           "n_records": int(db.n), "n_residues": int(db.total),
+                           "rank0_records": [searcher.begin, searcher.end],
+                           "rank0_residues": local_res, "merge": "all_gather of k hits per query"},
+            }
+        return line, merged
+    finally:
+        if on_gpu:
+            ctx.close()
+
+
+def main(argv=None):
+    args = parse(argv)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
@@ -688,6 +760,18 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local_rank)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    if args.shard:
+        if world == 1:
+            import torch.distributed as dist
+            dist.init_process_group("nccl", init_method="tcp://127.0.0.1:29533", rank=0,
+                                    world_size=1)
+        line, _ = run_shard(args, rank, world, local_rank)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+        return 0
     line, db, queries, gpu_scores = run_ours(args, rank, world, local_rank)
     if line is None:
         return 0

@@ -8,6 +8,8 @@
 // include/swb200.h.  Header-only; link with -lswb200 -lpthread.
 #pragma once
 
+#include <algorithm>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -297,18 +299,41 @@ private:
 };
 
 // ---------------------------------------------------------------------------
+// Residue-balanced split of one DB over n devices: contiguous record ranges
+// [cut[g], cut[g+1]) with about the same number of residues each.  Cut g is
+// the first record whose start offset reaches g/n of the residues (the rule
+// of shard_bounds in swhybrid_b200/shard.py), never before the previous cut.
+// ---------------------------------------------------------------------------
+inline std::vector<size_t> shard_bounds(const std::vector<uint64_t>& offsets, int n) {
+    const size_t nrec = offsets.empty() ? 0 : offsets.size() - 1;
+    std::vector<size_t> cuts(1, 0);
+    if (n < 1) n = 1;
+    const uint64_t base = nrec ? offsets[0] : 0, total = nrec ? offsets[nrec] - base : 0;
+    for (int g = 1; g < n; ++g) {
+        const uint64_t target = base + (uint64_t)((unsigned __int128)total * g / n);
+        size_t c = (size_t)(std::lower_bound(offsets.begin(), offsets.end(), target) -
+                            offsets.begin());
+        c = std::min(std::max(c, cuts.back()), nrec);
+        cuts.push_back(c);
+    }
+    cuts.push_back(nrec);
+    return cuts;
+}
+
+// ---------------------------------------------------------------------------
 // WorkerPool (src/WorkerPool.cpp:10-155): one B200Worker per GPU, each on its
-// own thread, over a slice of the records; results merged into one list.
+// own thread, over a residue-balanced slice of the records; results merged
+// into one list.
 // ---------------------------------------------------------------------------
 class WorkerPool {
 public:
     WorkerPool(DataPool* loader, Param* params) : loader(loader), params(params),
                                                   resultList(params->topNum) {
         const int n = std::max(1, params->cudaNum);
-        const size_t nrec = loader->offsets.size() - 1;
+        const std::vector<size_t> cuts = shard_bounds(loader->offsets, n);
         for (int g = 0; g < n; ++g) {
             // records [b, e) of the input order go to GPU g
-            const size_t b = nrec * g / n, e = nrec * (g + 1) / n;
+            const size_t b = cuts[g], e = cuts[g + 1];
             DataPool* part = new DataPool();
             part->query = loader->query;
             part->offsets.assign(1, 0);

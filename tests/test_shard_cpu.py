@@ -77,3 +77,88 @@ def test_shard_bounds_balance_and_cover():
         sizes = [int(off[e] - off[s]) for s, e in b]
         assert max(sizes) - min(sizes) <= 2 * int(lens.max())
     assert shard.shard_bounds(np.zeros(1, dtype=np.int64), 4) == [(0, 0)] * 4
+
+
+def test_cpp_worker_pool_split_equals_shard_bounds():
+    """The C++ WorkerPool (swhybrid_b200/cpp/swb200_worker.hpp) splits by
+    residues with the same rule: on a DB sorted longest first, a split by
+    record count would give the first device most of the residues."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = os.path.join(root, "swhybrid_b200", "cpp", "shard_bounds_test")
+    rng = np.random.default_rng(8)
+    lens = np.sort(rng.lognormal(5.6, 0.7, size=5000).astype(np.int64) + 1)[::-1]
+    cases = [lens, rng.integers(0, 3000, size=777), np.zeros(5, dtype=np.int64),
+             np.array([100000] + [1] * 50, dtype=np.int64)]
+    for L in cases:
+        off = np.zeros(len(L) + 1, dtype=np.int64)
+        off[1:] = np.cumsum(L)
+        for world in (1, 2, 3, 4, 8):
+            out = subprocess.run([exe, str(world)], input=" ".join(map(str, off)),
+                                 capture_output=True, text=True, check=True).stdout.split()
+            cuts = [int(x) for x in out]
+            want = shard.shard_bounds(off, world)
+            assert [(cuts[i], cuts[i + 1]) for i in range(world)] == want
+    off = np.zeros(len(lens) + 1, dtype=np.int64)
+    off[1:] = np.cumsum(lens)
+    (b0, e0), (b1, e1) = shard.shard_bounds(off, 2)
+    assert abs(int(off[e0] - off[b0]) - int(off[e1] - off[b1])) <= int(lens.max())
+    assert e0 < len(lens) // 2          # the long records sit in the first half
+
+
+class _OracleCtx:
+    """Stands in for a device context in the CPU test of bench.py --shard:
+    the oracle scores the rank's shard."""
+
+    class _P:
+        top_k = K
+
+    params = _P()
+
+    def load_db(self, res, off):
+        self.res, self.off = np.asarray(res), np.asarray(off)
+
+    def search(self, q):
+        sc, idx = oracle.topk(oracle.search(q, self.res, self.off, param.blosum62(), 12, 2), K)
+        return list(zip(sc.tolist(), idx.tolist())), None
+
+
+def shard_bench_worker(rank, world, port, out):
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        import bench
+        res, off, q = make_case()
+
+        class _DB:
+            residues, offsets = res, off
+            n = len(off) - 1
+            total = int(off[-1])
+
+        args = bench.parse(["--shard", "--steps", "2", "--warmup", "1", "--workload", "small"])
+        line, merged = bench.run_shard(args, rank, world, 0, make_ctx=_OracleCtx,
+                                       workload=(_DB, [q, q[:50]]))
+        out[rank] = (line, merged)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_bench_shard_mode_two_ranks_equals_whole_db():
+    """bench.py --shard on two gloo ranks: each rank searches its residue-
+    balanced slice, one all-gather per query merges the k best hits; the
+    merged lists equal the whole-DB top-k and rank 0 reports the line."""
+    world = 2
+    with mp.get_context("spawn").Manager() as m:
+        out = m.dict()
+        mp.spawn(shard_bench_worker, args=(world, free_port(), out), nprocs=world, join=True)
+        got = dict(out)
+    res, off, q = make_case()
+    for qq, i in ((q, 0), (q[:50], 1)):
+        sc, idx = oracle.topk(oracle.search(qq, res, off, param.blosum62(), 12, 2), K)
+        want = list(zip(sc.tolist(), idx.tolist()))
+        assert got[0][1][i] == want and got[1][1][i] == want
+    line = got[0][0]
+    assert got[1][0] is None
+    assert line["scaling"] == "strong" and line["n_gpus"] == 2 and line["value"] > 0
+    assert line["config"]["rank0_records"][0] == 0
