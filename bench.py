@@ -71,6 +71,8 @@ def parse(argv=None):
                     help="skip the batched (64-query) measurement")
     ap.add_argument("--serve-requests", type=int, default=96,
                     help="requests per offered load in the serving leg (0 = skip it)")
+    ap.add_argument("--serve-levels", type=str, default="0.25,0.5,0.75,1.0",
+                    help="offered loads of the serving leg, as fractions of the saturating rate")
     ap.add_argument("--no-stress", action="store_true",
                     help="skip the overflow / long-record stress measurement")
     ap.add_argument("--kernel-only", action="store_true",
@@ -300,7 +302,7 @@ def run_reference(args, rank, world):
 
 
 # ---------------------------------------------------------------------------
-def serve_leg(ctx, db, n_req: int, seed: int = 5):
+def serve_leg(ctx, db, n_req: int, seed: int = 5, levels=(0.25, 0.5, 0.75, 1.0)):
     """Serving: requests of lengths log-uniform 30..8,000 (seeded) against the
     resident DB through sw_serve_*.  First the saturating rate (3x the slot
     count submitted at once), then Poisson arrivals at 25/50/75/100% of it,
@@ -336,7 +338,7 @@ def serve_leg(ctx, db, n_req: int, seed: int = 5):
         check_ids = []
         base = 1_000_000
         level_qs = requests(n_req)           # the same requests at every offered load
-        for frac in (0.25, 0.5, 0.75, 1.0):
+        for frac in levels:
             qs = level_qs
             arr = _synth.poisson_arrivals(rng, n_req, frac * sat_rate)
             st0 = ctx.serve_stats()
@@ -377,7 +379,8 @@ def serve_leg(ctx, db, n_req: int, seed: int = 5):
     return {
         "workload": "requests of lengths log-uniform 30..8,000 (seeded) against the full-size DB; "
                     "saturating rate from %d requests queued at once, then Poisson arrivals at "
-                    "25/50/75/100%% of it, the same %d requests at every level" % (3 * slots, n_req),
+                    "%s%% of it, the same %d requests at every level" % (
+                        3 * slots, "/".join(f"{100 * f:g}" for f in levels), n_req),
         "slots": slots, "chunks": int(st.chunks),
         "saturated": {"requests": len(sat_q), "rate_per_s": round(sat_rate, 3),
                       "gcups": round(sat_cells / ((t1 - t0) * 1e-3) / 1e9, 1)},
@@ -589,7 +592,8 @@ def run_ours(args, rank, world, local_rank):
     served = None
     if args.workload == "full" and args.serve_requests > 0:
         ctx.set_stream(None)
-        served = serve_leg(ctx, db, args.serve_requests)
+        served = serve_leg(ctx, db, args.serve_requests,
+                           levels=tuple(float(x) for x in args.serve_levels.split(",")))
 
     # ---- overflow / long-record stress (its own DB and context) ----
     stress = None
@@ -668,6 +672,14 @@ def run_ours(args, rank, world, local_rank):
         if spot is not None:
             line["parity_spot_check"] = spot
         if batched is not None:
+            # most of the batch runs two queries per register (no per-row byte
+            # unpacking): its roofline is that cell's measured mix
+            pm = rates.get("cell_pair_mix_gcups")
+            batched["roofline"] = {
+                "bound": "int_alu (packed int16x2 DPX, paired queries)",
+                "achieved": batched["value"], "peak": round(pm, 1) if pm else None,
+                "unit": "GCUPS", "frac": round(batched["value"] / pm, 4) if pm else None,
+                "peak_source": "measured live: libswprobe paired-query cell mix"}
             line["batched"] = batched
         if served is not None:
             line["served"] = served

@@ -228,7 +228,11 @@ sw_status sw_db_title(const struct sw_ctx *ctx, uint64_t record, const char **ti
  * plus the RecalcWorker pass (src/RecalcWorker.cpp:99-268) plus the top-k
  * merge (src/ResultList.h:37-79, src/WorkerPool.cpp:99-105).
  * hits: top_k entries; *n_hits receives how many have score > 0.
- * scores: optional (NULL or n_records int32), every record's score in DB order. */
+ * scores: optional (NULL or n_records int32), every record's score in DB order.
+ * Any query length: a query whose profile does not fit one block's shared
+ * memory (over ~8,000 residues with the wide shapes) is scored in row
+ * segments of whole passes by consecutive launches, each handing its last
+ * row (H and F per column) to the next, with the scores merged by maximum. */
 sw_status sw_search(struct sw_ctx *ctx, const uint8_t *query, uint32_t qlen,
                     sw_hit *hits, uint32_t *n_hits, int32_t *scores);
 
@@ -390,11 +394,16 @@ typedef struct sw_serve_options {
     int32_t group_width;      /* kernel shape of the rounds */
     int32_t rows_per_thread;
     int32_t stack_rows;       /* requests shorter than this share stacks */
+    int32_t pair_rows;        /* requests of at most this many residues are scored two
+                                 per register (paired lanes, as in sw_search_batch) with
+                                 shape pair_group_width x pair_rows_per_thread; 0 = off */
+    int32_t pair_group_width;
+    int32_t pair_rows_per_thread;
 } sw_serve_options;
 
 /* Defaults: 128 slots, 4 chunks, unbounded queue, half the free memory,
- * shape 16x64, stacks of 4096 rows (the best saturated throughput measured
- * on B200 for requests of 30..8,000 residues against a 205 M-residue DB). */
+ * shape 16x64, stacks of 4096 rows, requests of up to 2048 residues paired
+ * two per register with shape 16x64 (as sw_search_batch does). */
 void sw_serve_options_default(sw_serve_options *opt);
 
 typedef struct sw_serve_result {
@@ -419,8 +428,12 @@ typedef struct sw_serve_stats {
  * min(max_active, memory_budget / bytes per request in flight). */
 sw_status sw_serve_start(struct sw_ctx *ctx, const sw_serve_options *opt);
 
-/* Queues a request (codes 0..24, 1..8192 residues).  SW_ERR_BUSY when
- * max_pending requests already wait; SW_ERR_STATE when not serving. */
+/* Queues a request (codes 0..24, 1..2^24 residues).  SW_ERR_BUSY when
+ * max_pending requests already wait; SW_ERR_STATE when not serving.  A
+ * request longer than one stack of the serving shape holds (8,192 rows for
+ * the default 16 x 64; its query profile must fit one block's shared memory)
+ * is scored alone at a round boundary by the plain path, which splits its
+ * rows over consecutive launches, instead of sharing the round's launches. */
 sw_status sw_serve_submit(struct sw_ctx *ctx, uint64_t request_id, const uint8_t *query,
                           uint32_t qlen);
 

@@ -94,8 +94,7 @@ class sw_serve_options(ctypes.Structure):
                 ("max_pending", ctypes.c_uint32), ("memory_budget", ctypes.c_uint64),
                 ("group_width", ctypes.c_int32), ("rows_per_thread", ctypes.c_int32),
                 ("stack_rows", ctypes.c_int32), ("pair_rows", ctypes.c_int32),
-                ("pair_group_width", ctypes.c_int32), ("pair_rows_per_thread", ctypes.c_int32),
-                ("pair_long", ctypes.c_int32)]
+                ("pair_group_width", ctypes.c_int32), ("pair_rows_per_thread", ctypes.c_int32)]
 
 
 class sw_serve_result(ctypes.Structure):
@@ -511,7 +510,7 @@ class Context:
 
     # ---- serving ----------------------------------------------------------
     def serve_start(self, max_active=None, chunks=None, max_pending=None, memory_budget=None,
-                    shape=None, stack_rows=None):
+                    shape=None, stack_rows=None, pair_rows=None, pair_shape=None):
         o = sw_serve_options()
         self.L.sw_serve_options_default(ctypes.byref(o))
         if max_active is not None:
@@ -526,6 +525,10 @@ class Context:
             o.group_width, o.rows_per_thread = shape
         if stack_rows is not None:
             o.stack_rows = stack_rows
+        if pair_rows is not None:
+            o.pair_rows = pair_rows
+        if pair_shape is not None:
+            o.pair_group_width, o.pair_rows_per_thread = pair_shape
         self._check(self.L.sw_serve_start(self.h, ctypes.byref(o)), "sw_serve_start")
 
     def serve_submit(self, request_id: int, query: np.ndarray) -> int:

@@ -59,7 +59,7 @@ struct StackPlan {
     std::vector<int32_t> qp_rb_map;       // pairs of entries
 };
 
-const QpKernel* find_qp(int T, int R) {
+const QpKernel* swb::find_qp(int T, int R) {
     int n = 0;
     const QpKernel* q = qp_kernels(&n);
     for (int i = 0; i < n; ++i)

@@ -33,8 +33,10 @@ struct WfArgs {
     const Pair2* pairs;         // pair table, ncols descending
     int pair_begin;             // first pair handled by this launch
     int pair_count;             // pairs handled by this launch
-    const uint8_t* query;       // device query codes, qlen entries (< 25)
+    const uint8_t* query;       // device query codes of this launch's rows, qlen entries (< 25)
     int qlen;
+    int pass0;                  // query passes scored by earlier launches (row segments)
+    int more;                   // != 0: a later launch scores the next row segment
     const int8_t* mat;          // 32x32, [query code][db code]; codes >= 24 score 0
     uint32_t bias2;             // dup16(open+extend): the biased zero of a lane
     uint32_t neg_e;             // dup16(-extend)

@@ -447,6 +447,19 @@ int shape_occupancy(sw_ctx* ctx, const WfKernel& k, int qlen) {
     return nb;
 }
 
+// Query rows one launch of a shape scores: the whole query when its profile
+// fits one block, else the most whole passes whose profile does (a longer
+// query is scored in row segments by consecutive launches that hand the
+// boundary row on); 0 when not even one pass fits.
+int launch_rows(sw_ctx* ctx, const WfKernel& k, int qlen) {
+    if (shape_occupancy(ctx, k, qlen) > 0) return qlen;
+    const int rows_pass = k.T * k.R;
+    int p = 0;
+    while ((int64_t)(p + 1) * rows_pass < qlen && shape_occupancy(ctx, k, (p + 1) * rows_pass) > 0)
+        ++p;
+    return p * rows_pass;
+}
+
 // Sum over the pairs [b, e) of max(ncols, m): the column steps of one pass
 // whose segments last at least m steps.  Pairs are sorted by ncols
 // descending, so the pairs below m are a suffix of the range.
@@ -466,7 +479,8 @@ double cols_at_least(const sw_ctx* ctx, int64_t b, int64_t e, uint32_t m) {
 // on average there.  Columns per pass are counted as the streaming loop runs
 // them: at least 2T + 2 steps for a pass a later pass depends on, 3 otherwise.
 double shape_cost(sw_ctx* ctx, const WfKernel& k, int qlen, int64_t b, int64_t e) {
-    const int occ = shape_occupancy(ctx, k, qlen);
+    const int rows = launch_rows(ctx, k, qlen);
+    const int occ = rows > 0 ? shape_occupancy(ctx, k, rows) : 0;
     if (occ == 0 || e <= b) return occ == 0 ? 1e300 : 0.0;
     const double P = (qlen + k.T * k.R - 1) / (k.T * k.R);
     const double cols = (P - 1) * cols_at_least(ctx, b, e, 2 * k.T + 2) + cols_at_least(ctx, b, e, 3);
@@ -693,10 +707,10 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
         if (sg.e <= sg.b) continue;
         const WfKernel* k = find_kernel(sg.T, sg.R);
         if (!k) SW_SET(ctx, SW_ERR_INVALID, "no kernel %dx%d", sg.T, sg.R);
-        if (shape_occupancy(ctx, *k, qlen) == 0)
+        if (launch_rows(ctx, *k, qlen) == 0)
             SW_SET(ctx, SW_ERR_UNSUPPORTED,
-                   "query of %d residues does not fit shape %dx%d (profile %zu bytes)", qlen,
-                   sg.T, sg.R, k->smem(qlen));
+                   "one pass of shape %dx%d does not fit shared memory (profile %zu bytes)",
+                   sg.T, sg.R, k->smem(sg.T * sg.R));
     }
     // the search's timing events, taken after every check (a refused search
     // holds none), then its buffers cleared
@@ -763,39 +777,50 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
         if (sg.e <= sg.b) continue;
         const WfKernel* k = find_kernel(sg.T, sg.R);
         if (!k) SW_SET(ctx, SW_ERR_INVALID, "no kernel %dx%d", sg.T, sg.R);
-        const int occ = shape_occupancy(ctx, *k, qlen);
-        if (occ == 0)
+        // rows per launch: the whole query, or row segments of whole passes
+        // scored by consecutive launches (boundary row handed on, scores
+        // merged by maximum)
+        const int seg_rows = launch_rows(ctx, *k, qlen);
+        if (seg_rows == 0)
             SW_SET(ctx, SW_ERR_UNSUPPORTED,
-                   "query of %d residues does not fit shape %dx%d (profile %zu bytes)", qlen,
-                   sg.T, sg.R, k->smem(qlen));
-        WfArgs a;
-        a.db = ctx->d_db;
-        a.pairs = ctx->d_pairs;
-        a.pair_begin = (int)sg.b;
-        a.pair_count = (int)(sg.e - sg.b);
-        a.query = d_query;
-        a.qlen = qlen;
-        a.mat = ctx->d_mat;
-        a.bias2 = (uint32_t)(ctx->params.gap_open + ctx->params.gap_extend);
-        a.bias2 |= a.bias2 << 16;
-        a.neg_e = (uint32_t)(uint16_t)(int16_t)(-ctx->params.gap_extend);
-        a.neg_e |= a.neg_e << 16;
-        a.counter = ctx->d_counters + sg.counter;
-        a.bnd = ctx->d_bnd;
-        a.scores = ctx->d_scores;
-        a.n_records = (int)ctx->n_records;
-        a.ovf_list = ctx->d_ovf;
-        a.ovf_count = ctx->d_counters + 2;
-        a.ovf_thresh = ovf_thresh;
-        void* args[] = {&a};
-        int64_t grid = (int64_t)occ * (ctx->num_sms - reserved_sms);
-        const int64_t groups_per_block = k->block / k->T;
-        grid = std::min<int64_t>(grid, ((sg.e - sg.b) + groups_per_block - 1) / groups_per_block);
-        grid = std::max<int64_t>(grid, 1);
-        SW_CUDA(ctx, cudaLaunchKernel(k->fn, dim3((unsigned)grid), dim3(k->block), args,
-                                      k->smem(qlen), st));
-        ++*launches;
-        ++mk.fp_launches;
+                   "one pass of shape %dx%d does not fit shared memory (profile %zu bytes)",
+                   sg.T, sg.R, k->smem(sg.T * sg.R));
+        for (int r0 = 0; r0 < qlen; r0 += seg_rows) {
+            const int rows = std::min(seg_rows, qlen - r0);
+            const int occ = shape_occupancy(ctx, *k, rows);
+            if (r0 > 0)   // the previous segment's launch has claimed every pair
+                SW_CUDA(ctx, cudaMemsetAsync(ctx->d_counters + sg.counter, 0, sizeof(int), st));
+            WfArgs a;
+            a.db = ctx->d_db;
+            a.pairs = ctx->d_pairs;
+            a.pair_begin = (int)sg.b;
+            a.pair_count = (int)(sg.e - sg.b);
+            a.query = d_query + r0;
+            a.qlen = rows;
+            a.pass0 = r0 / (k->T * k->R);
+            a.more = r0 + rows < qlen ? 1 : 0;
+            a.mat = ctx->d_mat;
+            a.bias2 = (uint32_t)(ctx->params.gap_open + ctx->params.gap_extend);
+            a.bias2 |= a.bias2 << 16;
+            a.neg_e = (uint32_t)(uint16_t)(int16_t)(-ctx->params.gap_extend);
+            a.neg_e |= a.neg_e << 16;
+            a.counter = ctx->d_counters + sg.counter;
+            a.bnd = ctx->d_bnd;
+            a.scores = ctx->d_scores;
+            a.n_records = (int)ctx->n_records;
+            a.ovf_list = ctx->d_ovf;
+            a.ovf_count = ctx->d_counters + 2;
+            a.ovf_thresh = ovf_thresh;
+            void* args[] = {&a};
+            int64_t grid = (int64_t)occ * (ctx->num_sms - reserved_sms);
+            const int64_t groups_per_block = k->block / k->T;
+            grid = std::min<int64_t>(grid, ((sg.e - sg.b) + groups_per_block - 1) / groups_per_block);
+            grid = std::max<int64_t>(grid, 1);
+            SW_CUDA(ctx, cudaLaunchKernel(k->fn, dim3((unsigned)grid), dim3(k->block), args,
+                                          k->smem(rows), st));
+            ++*launches;
+            ++mk.fp_launches;
+        }
     }
     if (split) {
         SW_CUDA(ctx, cudaEventRecord(mk.e[7], st));
@@ -916,6 +941,13 @@ extern "C" sw_status sw_search(sw_ctx* ctx, const uint8_t* query, uint32_t qlen,
                                uint32_t* n_hits, int32_t* scores) {
     if (!ctx) return SW_ERR_INVALID;
     if (ctx->serve) return SW_ERR_BUSY;   // the serving loop owns the stream and the DB
+    return swb::search_host(ctx, query, qlen, hits, n_hits, scores);
+}
+
+namespace swb {
+
+sw_status search_host(sw_ctx* ctx, const uint8_t* query, uint32_t qlen, sw_hit* hits,
+                      uint32_t* n_hits, int32_t* scores) {
     if (!ctx->db_loaded) SW_SET(ctx, SW_ERR_STATE, "no DB loaded (call sw_db_load first)");
     if ((qlen && !query) || (!hits && ctx->params.top_k > 0) || !n_hits)
         SW_SET(ctx, SW_ERR_INVALID, "null argument");
@@ -973,6 +1005,8 @@ extern "C" sw_status sw_search(sw_ctx* ctx, const uint8_t* query, uint32_t qlen,
     ctx->stats.total_ms = now_ms() - t0;
     return SW_OK;
 }
+
+}  // namespace swb
 
 extern "C" sw_status sw_search_device(sw_ctx* ctx, const uint8_t* d_query, uint32_t qlen,
                                       int32_t* d_scores) {

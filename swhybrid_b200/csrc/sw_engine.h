@@ -118,6 +118,11 @@ namespace swb {
 struct WfKernel;
 const WfKernel* find_kernel(int T, int R);
 int shape_occupancy(sw_ctx* ctx, const WfKernel& k, int qlen);
+int launch_rows(sw_ctx* ctx, const WfKernel& k, int qlen);
+// sw_search without the serving check: one plain search with host buffers
+// (the serving scheduler runs requests too long for a stack through it)
+sw_status search_host(sw_ctx* ctx, const uint8_t* query, uint32_t qlen, sw_hit* hits,
+                      uint32_t* n_hits, int32_t* scores);
 sw_kernel_config choose_config(sw_ctx* ctx, int qlen);
 sw_status take_marks(sw_ctx* ctx, sw_ctx::Marks* m);
 sw_status drain(sw_ctx* ctx, float* last_ms, float* last_fp_ms);

@@ -127,6 +127,35 @@ __device__ __forceinline__ void reverse_sweep_qp(uint32_t (&H)[R], const uint32_
     }
 }
 
+// One column step of a thread's two halves with packed profile words: the
+// top half (rows [0, R/2)) on column c at pt, the bottom half on column c - 1
+// at pb (see column_step in sw_wavefront.cuh for the carried values).
+template <int R, int JSTRIDE>
+__device__ __forceinline__ void column_step_qp(uint32_t (&H)[R], uint32_t (&E)[R],
+                                               const uint4* pt, const uint4* pb,
+                                               uint32_t prev_h, uint32_t f_in,
+                                               uint32_t& mid_h, uint32_t& mid_f,
+                                               uint32_t& out_h, uint32_t& out_f,
+                                               uint32_t& S_top, uint32_t& S_bot,
+                                               const CellK& K) {
+    constexpr int HALF = R / 2;
+    const uint32_t bot_diag = mid_h;
+    uint32_t f_top = f_in, f_bot = mid_f;
+    mid_h = H[HALF - 1];
+    reverse_sweep_qp<R, 0, HALF>(H, E, pt, JSTRIDE, prev_h);
+    reverse_sweep_qp<R, HALF, R>(H, E, pb, JSTRIDE, bot_diag);
+#pragma unroll
+    for (int i = 0; i < HALF; ++i) {
+        forward_cell(H[i], E[i], f_top, K);
+        forward_cell(H[HALF + i], E[HALF + i], f_bot, K);
+        if (i & 1) S_top = __vimax3_s16x2(S_top, H[i - 1], H[i]);
+        if (i & 1) S_bot = __vimax3_s16x2(S_bot, H[HALF + i - 1], H[HALF + i]);
+    }
+    mid_f = f_top;
+    out_h = H[R - 1];
+    out_f = f_bot;
+}
+
 // One double stack: every group claims units (records) and scores them
 // against both lanes' stacks.  Returns when the units are exhausted.  The
 // groups stream from pass to pass and unit to unit without draining, as in
@@ -267,23 +296,9 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
         h_in = (h_in & ~reset) | (Z & reset);
         f_in = (f_in & ~reset) | (Z & reset);
         if (!fin && c >= 0) {
-            const uint4* pt = prof_t + (int)d_in * SLOTS;
-            const uint4* pb = prof_b + (int)d_bot * SLOTS;
-            const uint32_t bot_diag = mid_h;
-            uint32_t f_top = f_in, f_bot = mid_f;
-            mid_h = H[HALF - 1];
-            reverse_sweep_qp<R, 0, HALF>(H, E, pt, JSTRIDE, prev_h);
-            reverse_sweep_qp<R, HALF, R>(H, E, pb, JSTRIDE, bot_diag);
-#pragma unroll
-            for (int i = 0; i < HALF; ++i) {
-                forward_cell(H[i], E[i], f_top, K);
-                forward_cell(H[HALF + i], E[HALF + i], f_bot, K);
-                if (i & 1) S_top = __vimax3_s16x2(S_top, H[i - 1], H[i]);
-                if (i & 1) S_bot = __vimax3_s16x2(S_bot, H[HALF + i - 1], H[HALF + i]);
-            }
-            mid_f = f_top;
-            out_h = H[R - 1];
-            out_f = f_bot;
+            column_step_qp<R, JSTRIDE>(H, E, prof_t + (int)d_in * SLOTS,
+                                       prof_b + (int)d_bot * SLOTS, prev_h, f_in, mid_h, mid_f,
+                                       out_h, out_f, S_top, S_bot, K);
             if (t == T - 1 && b_col >= 0 && b_col < b_wlim)
                 b_wrow[2 * b_col] = make_uint2(out_h, out_f);
         }
@@ -382,6 +397,51 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
             }
         }
         ++c;
+
+        // Plain steps, as in run_stream: as many as every lane of the warp can
+        // take with no segment event and no bounds guard.  The bottom half's
+        // profile base is then the top's, so it takes the top's residue of
+        // the step before; the residue is loaded as the unit's own byte.
+        {
+            int k = 0;
+            if (!fin && c >= 1 && !(t == 0 && pass == 0 && c <= (nst < 9 ? nst - 1 : 8))) {
+                const int lastc = min(nst - 2, ncols - 3);
+                k = max(lastc - c + 1, 0);
+            }
+            k = (int)__reduce_min_sync(FULL, (unsigned)k);
+            const bool rd0 = t == 0 && has_in;
+            const bool z0 = t == 0 && !has_in;
+            const bool wr = t == T - 1 && wlim > 0;
+            const uint32_t keep = ~reset, zr = Z & reset;
+            const uint8_t* colb = reinterpret_cast<const uint8_t*>(col) + half;
+            for (; k > 0; --k) {
+                __syncwarp();
+                uint32_t h_in = __shfl_up_sync(FULL, out_h, 1, T);
+                uint32_t f_in = __shfl_up_sync(FULL, out_f, 1, T);
+                const uint32_t d_in = d_cur;
+                d_cur = (uint32_t)__ldg(colb + 2 * (c + 1));
+                if (rd0) {
+                    h_in = bq0.x;
+                    f_in = bq0.y;
+                    bq0 = bq1;
+                    bq1 = rrow[2 * (c + 2)];
+                }
+                if (z0) {
+                    h_in = Z;
+                    f_in = Z;
+                }
+                h_in = (h_in & keep) | zr;
+                f_in = (f_in & keep) | zr;
+                column_step_qp<R, JSTRIDE>(H, E, prof_t + (int)d_in * SLOTS,
+                                           prof_t + (int)d_bot * SLOTS, prev_h, f_in, mid_h,
+                                           mid_f, out_h, out_f, S_top, S_bot, K);
+                if (wr) wrow[2 * (c - 1)] = make_uint2(out_h, out_f);
+                prev_h = h_in;
+                d_bot = d_in;
+                b_col = c;
+                ++c;
+            }
+        }
     }
 #undef SWQ_SET_SEG
 }

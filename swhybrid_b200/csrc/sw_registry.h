@@ -23,5 +23,6 @@ struct QpKernel {
     size_t (*smem)(int rows);      // shared memory for a double stack of `rows` rows
 };
 const QpKernel* qp_kernels(int* n);
+const QpKernel* find_qp(int T, int R);     // null when that shape is not compiled
 
 }  // namespace swb

@@ -7,12 +7,17 @@
 //   * the DB's record pairs are dealt round-robin (longest first) into
 //     `chunks` chunks with the same length mix, and the chunks form a ring;
 //   * a device round scores the next chunk of the ring for every request in
-//     flight: one persistent launch of the stacked batched kernel (sw_batch)
-//     over all of them (short requests share R-row blocks of a stack, long
-//     ones get stacks of their own), one 32-bit re-score launch for the
-//     round's flagged (request, record) entries and, for the requests that
-//     have now seen every chunk, one top-k round sequence and the download
-//     of their keys;
+//     flight: short requests (up to pair_rows residues) two per register in
+//     paired lanes (one launch of sw_qpbatch, packed profile, as in
+//     sw_search_batch), the others in one persistent launch of the stacked
+//     kernel (sw_batch: short ones share R-row blocks of a stack, long ones
+//     get stacks of their own), one 32-bit re-score launch for the round's
+//     flagged (request, record) entries and, for the requests that have now
+//     seen every chunk, one top-k round sequence and the download of their
+//     keys;
+//   * rounds are pipelined: round r+1 is enqueued before the host waits for
+//     round r (double-buffered host tables, keys and overflow count), so the
+//     device does not idle while the host reads results and plans;
 //   * a request joins the ring at whatever chunk is next and completes after
 //     `chunks` rounds, so a request that arrives while a round runs waits at
 //     most that round before its work shares the device with everything
@@ -20,7 +25,11 @@
 //   * admission happens at every round boundary into free slots.  A slot is
 //     the device memory of one request in flight (its score row); the slot
 //     count is bounded by max_active and by a device-memory budget, and the
-//     waiting queue by max_pending (SW_ERR_BUSY beyond it).
+//     waiting queue by max_pending (SW_ERR_BUSY beyond it);
+//   * a request longer than one stack of the serving shape can hold (its
+//     query profile would not fit one block's shared memory) is scored alone
+//     at a round boundary by the plain path, which splits its rows over
+//     consecutive launches; it does not share launches with the batch.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -36,13 +45,14 @@
 #include "sw_aux.h"
 #include "sw_device.cuh"
 #include "sw_engine.h"
+#include "sw_qpair.cuh"
 #include "sw_registry.h"
 
 using namespace swb;
 
 namespace {
 
-constexpr uint32_t kServeMaxQuery = 8192;     // residues per request
+constexpr uint32_t kServeMaxQuery = 1u << 24;  // residues per request
 
 double now_ms() {
     return std::chrono::duration<double, std::milli>(
@@ -70,9 +80,13 @@ struct Slot {
 struct sw_serve_state {
     sw_serve_options opt{};
     const WfKernel* k = nullptr;
+    const QpKernel* qk = nullptr;         // paired lanes for short requests (null = off)
+    uint32_t pair_seg = 0;                // rows of a paired lane
     int n_slots = 0;
     int n_chunks = 1;
+    uint32_t max_stack_rows = 0;          // longer requests run alone (plain path)
     int occ_max = 0;                      // most blocks per SM any stack height gives
+    int occ_qp_max = 0;                   // ... and any paired lane height
     std::vector<int> chunk_begin;         // n_chunks + 1 entries into d_pairs
     Pair2* d_pairs = nullptr;             // pair table, chunk after chunk
     uint32_t* d_pair_ids = nullptr;       // global pair index of each entry
@@ -85,9 +99,13 @@ struct sw_serve_state {
     uint2* d_bnd = nullptr;
     size_t bnd_group = 0;
     unsigned long long* d_keys[2] = {nullptr, nullptr};
-    uint8_t* h_stage = nullptr;           // pinned: per-round tables
-    size_t stage_cap = 0;
-    unsigned long long* h_keys = nullptr; // pinned: n_slots * top_k
+    // per-round host buffers, two sets: round r+1 is enqueued before the host
+    // waits for round r, so r's tables, keys and flagged count stay untouched
+    uint8_t* h_stage[2] = {nullptr, nullptr};          // pinned: the round's tables
+    size_t stage_cap[2] = {0, 0};
+    unsigned long long* h_keys[2] = {nullptr, nullptr}; // pinned: n_slots * top_k
+    int* h_flagged[2] = {nullptr, nullptr};            // pinned: the round's overflow count
+    cudaEvent_t done_ev[2] = {nullptr, nullptr};       // the round's last operation
     int cursor = 0;                       // next chunk of the ring
     std::vector<Slot> slots;
     std::deque<Request> pending, done;
@@ -110,23 +128,31 @@ void serve_free(sw_serve_state* s) {
     dev_free(s->d_bnd);
     dev_free(s->d_keys[0]);
     dev_free(s->d_keys[1]);
-    if (s->h_stage) cudaFreeHost(s->h_stage);
-    if (s->h_keys) cudaFreeHost(s->h_keys);
-    s->h_stage = nullptr;
-    s->h_keys = nullptr;
+    for (int b = 0; b < 2; ++b) {
+        if (s->h_stage[b]) cudaFreeHost(s->h_stage[b]);
+        if (s->h_keys[b]) cudaFreeHost(s->h_keys[b]);
+        if (s->h_flagged[b]) cudaFreeHost(s->h_flagged[b]);
+        if (s->done_ev[b]) cudaEventDestroy(s->done_ev[b]);
+        s->h_stage[b] = nullptr;
+        s->h_keys[b] = nullptr;
+        s->h_flagged[b] = nullptr;
+        s->done_ev[b] = nullptr;
+        s->stage_cap[b] = 0;
+    }
 }
 
-// One device round: chunk `chunk` for every active slot.  `finishing` gets
-// the slots whose cycle ends with this round; their keys land in h_keys in
-// that order.  Runs on the scheduler thread only.
-sw_status run_round(sw_ctx* ctx, sw_serve_state* s, int chunk, std::vector<int>& finishing,
-                    uint32_t* launches, uint64_t* rescored) {
+// Enqueues one device round on the context's stream: chunk `chunk` for every
+// active slot, using host buffer set `buf`.  `finishing` gets the slots whose
+// cycle ends with this round; their keys land in h_keys[buf] in that order,
+// and the round's overflow count in h_flagged[buf], once done_ev[buf] has
+// completed.  Runs on the scheduler thread only.
+sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
+                        std::vector<int>& finishing, uint32_t* launches) {
     cudaStream_t st = ctx->stream;
     const int n_rec = (int)ctx->n_records;
     const int T = s->k->T, R = s->k->R;
     const uint32_t cap_rows = (uint32_t)std::max<int32_t>(s->opt.stack_rows, R);
     *launches = 0;
-    *rescored = 0;
     std::vector<int> active;
     finishing.clear();
     for (int i = 0; i < s->n_slots; ++i)
@@ -139,12 +165,21 @@ sw_status run_round(sw_ctx* ctx, sw_serve_state* s, int chunk, std::vector<int>&
     std::stable_sort(active.begin(), active.end(), [&](int a, int b) {
         return s->slots[a].req.query.size() > s->slots[b].req.query.size();
     });
+    // requests whose padded rows fit a paired lane: two per register against
+    // one record (sw_qpbatch, packed profile); the others: stacks
+    const QpKernel* qk = s->qk;
+    const uint32_t qR = qk ? (uint32_t)qk->R : 1u, qT = qk ? (uint32_t)qk->T : 1u;
+    std::vector<int> paired, stacked;
+    for (int sl : active) {
+        const uint32_t L = (uint32_t)s->slots[sl].req.query.size();
+        (qk && (L + qR - 1) / qR * qR <= s->pair_seg ? paired : stacked).push_back(sl);
+    }
     struct Stack {
         std::vector<int> slots;
         uint32_t rows = 0;
     };
     std::vector<Stack> stacks;
-    for (int sl : active) {
+    for (int sl : stacked) {
         const uint32_t L = (uint32_t)s->slots[sl].req.query.size();
         const uint32_t need = (L + R - 1) / R * R;
         bool placed = false;
@@ -195,28 +230,93 @@ sw_status run_round(sw_ctx* ctx, sw_serve_state* s, int chunk, std::vector<int>&
         for (uint32_t j = 0; j < P * (uint32_t)T; ++j)
             rbmap.push_back(j < block_q.size() ? block_q[j] : -1);
     }
-    const size_t o_qoff = 0, o_qlen = 4 * (size_t)s->n_slots, o_soff = 8 * (size_t)s->n_slots;
-    const size_t o_srows = o_soff + 4 * ns, o_rboff = o_srows + 4 * ns, o_rbmap = o_rboff + 4 * ns;
-    const size_t o_rows = o_rbmap + 4 * rbmap.size();
-    const size_t o_codes = o_rows + 4 * finishing.size();
-    const size_t total = (o_codes + codes.size() + 15) / 16 * 16;
+    // paired lanes: first fit (longest first) into lanes of at most pair_seg
+    // rows, each request padded to whole R-row blocks; consecutive lanes form
+    // a double stack (low lane, high lane)
+    struct Lane {
+        std::vector<int> slots;
+        uint32_t rows = 0;
+    };
+    std::vector<Lane> lanes;
+    for (int sl : paired) {
+        const uint32_t need = ((uint32_t)s->slots[sl].req.query.size() + qR - 1) / qR * qR;
+        bool placed = false;
+        for (Lane& ln : lanes)
+            if (ln.rows + need <= s->pair_seg) {
+                ln.slots.push_back(sl);
+                ln.rows += need;
+                placed = true;
+                break;
+            }
+        if (!placed) lanes.push_back(Lane{{sl}, need});
+    }
+    if (lanes.size() % 2) lanes.push_back(Lane{});
+    const size_t nd = lanes.size() / 2;
+    std::vector<uint32_t> qp_off[2], qp_rows[2], qp_rboff;
+    std::vector<int32_t> qp_rbmap;           // (low, high) entries
+    uint32_t qp_max_rows = 0;
+    for (size_t d = 0; d < nd; ++d) {
+        std::vector<int32_t> blocks[2];
+        for (int h = 0; h < 2; ++h) {
+            const Lane& ln = lanes[2 * d + h];
+            qp_off[h].push_back((uint32_t)codes.size());
+            qp_rows[h].push_back(ln.rows);
+            for (int sl : ln.slots) {
+                const std::vector<uint8_t>& q = s->slots[sl].req.query;
+                const uint32_t L = (uint32_t)q.size();
+                const uint32_t padded = (L + qR - 1) / qR * qR;
+                qoff[sl] = (uint32_t)codes.size();
+                qlen[sl] = L;
+                codes.insert(codes.end(), q.begin(), q.end());
+                codes.insert(codes.end(), padded - L, (uint8_t)kZeroCode);
+                for (uint32_t j = 0; j < padded / qR; ++j)
+                    blocks[h].push_back((int32_t)sl | (j == 0 ? kFirstBit : 0));
+            }
+        }
+        const uint32_t rows = std::max(lanes[2 * d].rows, lanes[2 * d + 1].rows);
+        qp_max_rows = std::max(qp_max_rows, rows);
+        const uint32_t P = std::max<uint32_t>(1, (rows + qT * qR - 1) / (qT * qR));
+        qp_rboff.push_back((uint32_t)(qp_rbmap.size() / 2));
+        for (uint32_t j = 0; j < P * qT; ++j)
+            for (int h = 0; h < 2; ++h)
+                qp_rbmap.push_back(j < blocks[h].size() ? blocks[h][j] : -1);
+    }
+    // table layout (one upload; the paired block map is read as int2)
+    size_t total = 0;
+    auto place = [&total](size_t bytes, size_t align) {
+        const size_t o = (total + align - 1) / align * align;
+        total = o + bytes;
+        return o;
+    };
+    const size_t o_qoff = place(4 * (size_t)s->n_slots, 4), o_qlen = place(4 * (size_t)s->n_slots, 4);
+    const size_t o_soff = place(4 * ns, 4), o_srows = place(4 * ns, 4), o_rboff = place(4 * ns, 4);
+    const size_t o_rbmap = place(4 * rbmap.size(), 4);
+    const size_t o_rows = place(4 * finishing.size(), 4);
+    const size_t o_qpo0 = place(4 * nd, 4), o_qpr0 = place(4 * nd, 4);
+    const size_t o_qpo1 = place(4 * nd, 4), o_qpr1 = place(4 * nd, 4), o_qprb = place(4 * nd, 4);
+    const size_t o_qpmap = place(4 * qp_rbmap.size(), 8);
+    const size_t o_codes = place(codes.size(), 16);
+    total = (total + 15) / 16 * 16;
     if (total > s->meta_cap) {
+        // the round in flight still reads the old tables
+        SW_CUDA(ctx, cudaStreamSynchronize(st));
         dev_free(s->d_meta);
         s->meta_cap = 0;
         if (dev_alloc(&s->d_meta, total * 2) != cudaSuccess)
             SW_SET(ctx, SW_ERR_NOMEM, "device allocation failed: serving tables");
         s->meta_cap = total * 2;
     }
-    if (total > s->stage_cap) {
-        // the previous round's upload has completed (every round ends synchronised)
-        if (s->h_stage) cudaFreeHost(s->h_stage);
-        s->h_stage = nullptr;
-        s->stage_cap = 0;
-        if (cudaMallocHost((void**)&s->h_stage, total * 2) != cudaSuccess)
+    if (total > s->stage_cap[buf]) {
+        // the round that last used this set has completed (the caller waits
+        // for it before reusing the set)
+        if (s->h_stage[buf]) cudaFreeHost(s->h_stage[buf]);
+        s->h_stage[buf] = nullptr;
+        s->stage_cap[buf] = 0;
+        if (cudaMallocHost((void**)&s->h_stage[buf], total * 2) != cudaSuccess)
             SW_SET(ctx, SW_ERR_NOMEM, "pinned allocation failed: serving tables");
-        s->stage_cap = total * 2;
+        s->stage_cap[buf] = total * 2;
     }
-    uint8_t* m = s->h_stage;
+    uint8_t* m = s->h_stage[buf];
     memcpy(m + o_qoff, qoff.data(), 4 * qoff.size());
     memcpy(m + o_qlen, qlen.data(), 4 * qlen.size());
     if (ns) {
@@ -226,6 +326,14 @@ sw_status run_round(sw_ctx* ctx, sw_serve_state* s, int chunk, std::vector<int>&
         memcpy(m + o_rbmap, rbmap.data(), 4 * rbmap.size());
     }
     if (!finishing.empty()) memcpy(m + o_rows, finishing.data(), 4 * finishing.size());
+    if (nd) {
+        memcpy(m + o_qpo0, qp_off[0].data(), 4 * nd);
+        memcpy(m + o_qpr0, qp_rows[0].data(), 4 * nd);
+        memcpy(m + o_qpo1, qp_off[1].data(), 4 * nd);
+        memcpy(m + o_qpr1, qp_rows[1].data(), 4 * nd);
+        memcpy(m + o_qprb, qp_rboff.data(), 4 * nd);
+        memcpy(m + o_qpmap, qp_rbmap.data(), 4 * qp_rbmap.size());
+    }
     if (!codes.empty()) memcpy(m + o_codes, codes.data(), codes.size());
     SW_CUDA(ctx, cudaMemcpyAsync(s->d_meta, m, total, cudaMemcpyHostToDevice, st));
     // score rows of requests admitted at this boundary start at zero (atomicMax)
@@ -233,12 +341,63 @@ sw_status run_round(sw_ctx* ctx, sw_serve_state* s, int chunk, std::vector<int>&
         if (s->slots[sl].fresh)
             SW_CUDA(ctx, cudaMemsetAsync(s->d_scores + (size_t)sl * n_rec, 0,
                                          (size_t)n_rec * sizeof(int), st));
-    SW_CUDA(ctx, cudaMemsetAsync(s->d_counters, 0, (ns + 1) * sizeof(int), st));
-    const int occ = std::min(shape_occupancy(ctx, *s->k, (int)max_rows), s->occ_max);
+    // counters: stack i at [i], the overflow count at [ns], double stack j at
+    // [ns + 1 + j]
+    SW_CUDA(ctx, cudaMemsetAsync(s->d_counters, 0, (ns + 1 + nd) * sizeof(int), st));
+    const int occ = ns ? std::min(shape_occupancy(ctx, *s->k, (int)max_rows), s->occ_max) : 1;
     if (occ <= 0)
         SW_SET(ctx, SW_ERR_UNSUPPORTED, "a stack of %u rows does not fit shape %dx%d", max_rows,
                T, R);
     int* d_ovf_count = s->d_counters + ns;
+    const int pair_count = s->chunk_begin[chunk + 1] - s->chunk_begin[chunk];
+    if (nd && pair_count > 0) {
+        const size_t smem = qk->smem((int)std::max<uint32_t>(qp_max_rows, 1));
+        int occq = 0;
+        if (smem > (size_t)ctx->max_smem ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occq, qk->fn, qk->block, smem) !=
+                cudaSuccess) {
+            cudaGetLastError();
+            occq = 0;
+        }
+        occq = std::min(occq, s->occ_qp_max);
+        if (occq <= 0)
+            SW_SET(ctx, SW_ERR_UNSUPPORTED, "paired lanes of %u rows do not fit shape %dx%d",
+                   qp_max_rows, qk->T, qk->R);
+        QpArgs q;
+        q.db = ctx->d_db;
+        q.pairs = s->d_pairs;
+        q.pair_begin = s->chunk_begin[chunk];
+        q.pair_count = pair_count;
+        q.codes = s->d_meta + o_codes;
+        q.off_lo = reinterpret_cast<const uint32_t*>(s->d_meta + o_qpo0);
+        q.rows_lo = reinterpret_cast<const uint32_t*>(s->d_meta + o_qpr0);
+        q.off_hi = reinterpret_cast<const uint32_t*>(s->d_meta + o_qpo1);
+        q.rows_hi = reinterpret_cast<const uint32_t*>(s->d_meta + o_qpr1);
+        q.rb_map = reinterpret_cast<const int2*>(s->d_meta + o_qpmap);
+        q.rb_off = reinterpret_cast<const uint32_t*>(s->d_meta + o_qprb);
+        q.nstacks = (int)nd;
+        q.counters = s->d_counters + ns + 1;
+        q.mat = ctx->d_mat;
+        q.bias2 = (uint32_t)(ctx->params.gap_open + ctx->params.gap_extend);
+        q.bias2 |= q.bias2 << 16;
+        q.neg_e = (uint32_t)(uint16_t)(int16_t)(-ctx->params.gap_extend);
+        q.neg_e |= q.neg_e << 16;
+        q.bnd = s->d_bnd;
+        q.bnd_group = s->bnd_group;
+        q.scores = s->d_scores;
+        q.n_records = n_rec;
+        q.ovf_list = s->d_ovf;
+        q.ovf_count = d_ovf_count;
+        q.ovf_thresh = 32767 - std::max(ctx->max_score, 1) + 1;
+        q.ovf_cap = (int)std::min<size_t>(s->ovf_cap, (size_t)INT32_MAX);
+        q.pair_ids = s->d_pair_ids;
+        q.seg_flags = nullptr;       // a paired lane is never cut into segments here
+        q.seg_bnd = s->d_bnd;
+        void* qargs[] = {&q};
+        SW_CUDA(ctx, cudaLaunchKernel(qk->fn, dim3((unsigned)(occq * ctx->num_sms)),
+                                      dim3(qk->block), qargs, smem, st));
+        ++*launches;
+    }
     {
         BatchArgs a;
         a.db = ctx->d_db;
@@ -267,7 +426,7 @@ sw_status run_round(sw_ctx* ctx, sw_serve_state* s, int chunk, std::vector<int>&
         a.ovf_cap = (int)std::min<size_t>(s->ovf_cap, (size_t)INT32_MAX);
         a.pair_ids = s->d_pair_ids;
         void* args[] = {&a};
-        if (a.pair_count > 0) {
+        if (a.pair_count > 0 && ns > 0) {
             SW_CUDA(ctx, cudaLaunchKernel(s->k->batch_fn, dim3((unsigned)(occ * ctx->num_sms)),
                                           dim3(s->k->block), args, s->k->smem((int)max_rows), st));
             ++*launches;
@@ -331,15 +490,24 @@ sw_status run_round(sw_ctx* ctx, sw_serve_state* s, int chunk, std::vector<int>&
             if (blocks == 1) break;
             n = blocks * (long long)k;
         }
-        SW_CUDA(ctx, cudaMemcpy2DAsync(s->h_keys, (size_t)k * sizeof(unsigned long long), keys_in,
+        SW_CUDA(ctx, cudaMemcpy2DAsync(s->h_keys[buf], (size_t)k * sizeof(unsigned long long), keys_in,
                                        (size_t)(nblk0 * kMaxTopK) * sizeof(unsigned long long),
                                        (size_t)k * sizeof(unsigned long long), finishing.size(),
                                        cudaMemcpyDeviceToHost, st));
     }
-    SW_CUDA(ctx, cudaStreamSynchronize(st));
+    SW_CUDA(ctx, cudaMemcpyAsync(s->h_flagged[buf], d_ovf_count, sizeof(int),
+                                 cudaMemcpyDeviceToHost, st));
+    SW_CUDA(ctx, cudaEventRecord(s->done_ev[buf], st));
     SW_CUDA(ctx, cudaGetLastError());
-    int flagged = 0;
-    SW_CUDA(ctx, cudaMemcpy(&flagged, d_ovf_count, sizeof(int), cudaMemcpyDeviceToHost));
+    return SW_OK;
+}
+
+// Waits for the round enqueued with buffer set `buf` and checks it; returns
+// its overflow count in *rescored.
+sw_status wait_round(sw_ctx* ctx, sw_serve_state* s, int buf, uint64_t* rescored) {
+    SW_CUDA(ctx, cudaEventSynchronize(s->done_ev[buf]));
+    SW_CUDA(ctx, cudaGetLastError());
+    const int flagged = *s->h_flagged[buf];
     if ((size_t)flagged > s->ovf_cap)
         SW_SET(ctx, SW_ERR_UNSUPPORTED, "%d overflow entries exceed the list (%zu)", flagged,
                s->ovf_cap);
@@ -347,17 +515,146 @@ sw_status run_round(sw_ctx* ctx, sw_serve_state* s, int chunk, std::vector<int>&
     return SW_OK;
 }
 
+// Requests longer than a stack: one plain search each (its rows split over
+// consecutive launches), at a round boundary, on the scheduler thread.
+void run_solo(sw_ctx* ctx, sw_serve_state* s, std::vector<Request>& reqs) {
+    const int k = ctx->params.top_k;
+    std::vector<sw_hit> hits((size_t)std::max(k, 1));
+    for (Request& r : reqs) {
+        const double t0 = now_ms();
+        uint32_t nh = 0;
+        const sw_status st = search_host(ctx, r.query.data(), (uint32_t)r.query.size(),
+                                         hits.data(), &nh, nullptr);
+        const double t1 = now_ms();
+        std::lock_guard<std::mutex> lock(s->mu);
+        r.start_ms = t0;
+        r.done_ms = t1;
+        r.status = st;
+        ++s->stats.admitted;
+        ++s->stats.rounds;
+        s->stats.launches += ctx->stats.launches;
+        s->stats.rescored += ctx->stats.rescored;
+        s->stats.busy_ms += t1 - t0;
+        if (st == SW_OK) {
+            r.hits.assign(hits.begin(), hits.begin() + nh);
+            s->stats.cells += (uint64_t)r.query.size() * ctx->n_residues;
+            ++s->stats.completed;
+        } else {
+            ++s->stats.failed;
+        }
+        s->done.push_back(std::move(r));
+        s->cv_done.notify_all();
+    }
+}
+
+// A round on the device whose results the host has not read yet.
+struct InFlight {
+    bool valid = false;
+    int buf = 0;                      // its host buffer set
+    std::vector<Request> leaving;     // requests whose cycle ends with it, in key order
+    double t_enq = 0;
+};
+
+// Hands out the requests of a completed (or failed) round.  Caller holds mu.
+void hand_out(sw_ctx* ctx, sw_serve_state* s, InFlight& r, sw_status st, double t1) {
+    const int k = ctx->params.top_k;
+    for (size_t f = 0; f < r.leaving.size(); ++f) {
+        Request& q = r.leaving[f];
+        q.done_ms = t1;
+        q.status = st;
+        if (st == SW_OK) {
+            for (int j = 0; j < k; ++j) {
+                const unsigned long long key = s->h_keys[r.buf][f * (size_t)k + j];
+                if (key == 0ull) break;
+                sw_hit h;
+                h.score = (int32_t)(key >> 32);
+                h.reserved = 0;
+                h.index = 0xffffffffull - (key & 0xffffffffull);
+                q.hits.push_back(h);
+            }
+            s->stats.cells += (uint64_t)q.query.size() * ctx->n_residues;
+            ++s->stats.completed;
+        } else {
+            q.hits.clear();
+            ++s->stats.failed;
+        }
+        s->done.push_back(std::move(q));
+    }
+    r.leaving.clear();
+    r.valid = false;
+}
+
+// Fails every request still holding a slot.  Caller holds mu.
+void fail_slots(sw_serve_state* s, sw_status st, double t1) {
+    for (Slot& x : s->slots) {
+        if (!x.used) continue;
+        x.req.done_ms = t1;
+        x.req.status = st;
+        x.req.hits.clear();
+        ++s->stats.failed;
+        s->done.push_back(std::move(x.req));
+        x.req = Request();
+        x.used = false;
+    }
+}
+
+// The scheduler thread.  Rounds are pipelined: round r+1 is enqueued (from the
+// slots' state after r, which is known when r is enqueued) before the host
+// waits for round r, so the device never idles while the host reads results
+// and builds the next round's tables.  A slot whose cycle ends with round r
+// is freed when r is enqueued: a request admitted into it clears its score
+// row on the stream after r's top-k has read it.
 void scheduler(sw_ctx* ctx) {
     sw_serve_state* s = ctx->serve;
     cudaSetDevice(ctx->device);
     std::vector<int> finishing;
+    std::vector<Request> solo;
+    InFlight prev;
+    int next_buf = 0;
+    double last_done = 0;
+    // waits for a round and hands its requests out; on failure every request
+    // in flight fails (the slots' score rows are no longer trustworthy)
+    auto complete = [&](InFlight& r) {
+        uint64_t rescored = 0;
+        const sw_status st = wait_round(ctx, s, r.buf, &rescored);
+        const double t1 = now_ms();
+        {
+            std::lock_guard<std::mutex> lock(s->mu);
+            s->stats.rescored += rescored;
+            s->stats.busy_ms += t1 - std::max(r.t_enq, last_done);
+            last_done = t1;
+            hand_out(ctx, s, r, st, t1);
+            if (st != SW_OK) fail_slots(s, st, t1);
+        }
+        s->cv_done.notify_all();
+        return st;
+    };
     while (true) {
         {
             std::unique_lock<std::mutex> lock(s->mu);
             bool any = false;
             for (const Slot& x : s->slots) any |= x.used;
-            if (!any)
+            if (!any && !prev.valid)
                 s->cv_work.wait(lock, [&] { return s->stopping || !s->pending.empty(); });
+            // requests too long for a stack leave the queue for the plain path
+            for (auto it = s->pending.begin(); it != s->pending.end();) {
+                if (it->query.size() > s->max_stack_rows) {
+                    solo.push_back(std::move(*it));
+                    it = s->pending.erase(it);
+                } else {
+                    ++it;
+                }
+            }
+        }
+        if (!solo.empty()) {
+            if (prev.valid) complete(prev);
+            run_solo(ctx, s, solo);
+            solo.clear();
+            continue;
+        }
+        bool any = false, stopping = false;
+        {
+            std::unique_lock<std::mutex> lock(s->mu);
             // admission: free slots take waiting requests, oldest first
             const double t_adm = now_ms();
             for (int i = 0; i < s->n_slots && !s->pending.empty(); ++i) {
@@ -371,59 +668,67 @@ void scheduler(sw_ctx* ctx) {
                 x.req.start_ms = t_adm;
                 ++s->stats.admitted;
             }
-            any = false;
             for (const Slot& x : s->slots) any |= x.used;
-            if (!any) {
-                if (s->stopping) break;
+            stopping = s->stopping;
+        }
+        if (!any) {
+            if (prev.valid) {
+                complete(prev);
                 continue;
             }
+            if (stopping) break;
+            continue;
         }
-        const double t0 = now_ms();
+        InFlight cur;
+        cur.valid = true;
+        cur.buf = next_buf;
+        cur.t_enq = now_ms();
         uint32_t launches = 0;
-        uint64_t rescored = 0;
-        const sw_status st = run_round(ctx, s, s->cursor, finishing, &launches, &rescored);
-        const double t1 = now_ms();
+        const sw_status est = enqueue_round(ctx, s, s->cursor, cur.buf, finishing, &launches);
         {
             std::lock_guard<std::mutex> lock(s->mu);
-            ++s->stats.rounds;
-            s->stats.launches += launches;
-            s->stats.rescored += rescored;
-            s->stats.busy_ms += t1 - t0;
-            const int k = ctx->params.top_k;
-            if (st == SW_OK)
-                for (size_t f = 0; f < finishing.size(); ++f) {
-                    Slot& x = s->slots[(size_t)finishing[f]];
-                    for (int j = 0; j < k; ++j) {
-                        const unsigned long long key = s->h_keys[f * (size_t)k + j];
-                        if (key == 0ull) break;
-                        sw_hit h;
-                        h.score = (int32_t)(key >> 32);
-                        h.reserved = 0;
-                        h.index = 0xffffffffull - (key & 0xffffffffull);
-                        x.req.hits.push_back(h);
+            if (est == SW_OK) {
+                ++s->stats.rounds;
+                s->stats.launches += launches;
+                for (int f : finishing) {
+                    Slot& x = s->slots[(size_t)f];
+                    cur.leaving.push_back(std::move(x.req));
+                    x.req = Request();
+                    x.used = false;
+                }
+                for (Slot& x : s->slots)
+                    if (x.used) {
+                        x.fresh = false;
+                        ++x.done_chunks;
                     }
-                }
-            for (Slot& x : s->slots) {
-                if (!x.used) continue;
-                x.fresh = false;
-                if (st == SW_OK && ++x.done_chunks < s->n_chunks) continue;
-                // cycle complete (its hits were read above), or the round failed
-                x.req.done_ms = t1;
-                x.req.status = st;
-                if (st == SW_OK) {
-                    s->stats.cells += (uint64_t)x.req.query.size() * ctx->n_residues;
-                    ++s->stats.completed;
-                } else {
-                    x.req.hits.clear();
-                    ++s->stats.failed;
-                }
-                s->done.push_back(std::move(x.req));
-                x.req = Request();
-                x.used = false;
+                s->cursor = (s->cursor + 1) % s->n_chunks;
             }
-            s->cursor = (s->cursor + 1) % s->n_chunks;
         }
-        s->cv_done.notify_all();
+        if (est != SW_OK) {
+            cudaStreamSynchronize(ctx->stream);
+            cudaGetLastError();
+            const double t1 = now_ms();
+            {
+                std::lock_guard<std::mutex> lock(s->mu);
+                if (prev.valid) hand_out(ctx, s, prev, est, t1);
+                fail_slots(s, est, t1);
+            }
+            s->cv_done.notify_all();
+            continue;
+        }
+        next_buf ^= 1;
+        if (prev.valid && complete(prev) != SW_OK) {
+            // the round just enqueued ran on failed state: drop it too
+            cudaEventSynchronize(s->done_ev[cur.buf]);
+            cudaGetLastError();
+            {
+                std::lock_guard<std::mutex> lock(s->mu);
+                hand_out(ctx, s, cur, SW_ERR_CUDA, now_ms());
+            }
+            s->cv_done.notify_all();
+            continue;
+        }
+        prev = std::move(cur);
     }
 }
 
@@ -458,6 +763,9 @@ extern "C" void sw_serve_options_default(sw_serve_options* o) {
     o->group_width = 16;
     o->rows_per_thread = 64;
     o->stack_rows = 4096;
+    o->pair_rows = 2048;
+    o->pair_group_width = 16;
+    o->pair_rows_per_thread = 64;
 }
 
 extern "C" sw_status sw_serve_start(sw_ctx* ctx, const sw_serve_options* opt) {
@@ -469,12 +777,17 @@ extern "C" sw_status sw_serve_start(sw_ctx* ctx, const sw_serve_options* opt) {
     sw_serve_options_default(&o);
     if (opt) o = *opt;
     const WfKernel* k = find_kernel(o.group_width, o.rows_per_thread);
-    if (!k || o.max_active == 0 || o.chunks == 0 || o.stack_rows < 0)
+    const QpKernel* qk = o.pair_rows > 0 ? find_qp(o.pair_group_width, o.pair_rows_per_thread)
+                                         : nullptr;
+    if (!k || o.max_active == 0 || o.chunks == 0 || o.stack_rows < 0 || o.pair_rows < 0 ||
+        (o.pair_rows > 0 && !qk))
         SW_SET(ctx, SW_ERR_INVALID, "bad serving options");
-    const int rows_big = (int)std::max<uint32_t>(kServeMaxQuery, (uint32_t)o.stack_rows);
-    if (shape_occupancy(ctx, *k, rows_big) == 0)
+    // the tallest stack the shape holds (whole passes whose profile fits one
+    // block); it must hold the configured stack height
+    const int max_stack_rows = launch_rows(ctx, *k, 1 << 30);
+    if (max_stack_rows < std::max(o.stack_rows, k->R))
         SW_SET(ctx, SW_ERR_UNSUPPORTED, "shape %dx%d cannot hold a stack of %d rows",
-               o.group_width, o.rows_per_thread, rows_big);
+               o.group_width, o.rows_per_thread, std::max(o.stack_rows, k->R));
     const int n_rec = (int)ctx->n_records;
     if ((uint64_t)o.max_active * (uint64_t)std::max(n_rec, 1) >= (1ull << 31))
         SW_SET(ctx, SW_ERR_UNSUPPORTED, "max_active x records reaches 2^31");
@@ -493,7 +806,27 @@ extern "C" sw_status sw_serve_start(sw_ctx* ctx, const sw_serve_options* opt) {
     s->opt = o;
     s->k = k;
     s->n_slots = (int)std::min<size_t>(o.max_active, budget / per_slot);
+    s->max_stack_rows = (uint32_t)max_stack_rows;
     s->occ_max = shape_occupancy(ctx, *k, k->R);
+    if (qk) {
+        const uint32_t pass_rows = (uint32_t)(qk->T * qk->R);
+        s->pair_seg = std::max(pass_rows, (uint32_t)o.pair_rows / pass_rows * pass_rows);
+        int occq = 0;
+        const size_t smem_seg = qk->smem((int)s->pair_seg);
+        if (smem_seg > (size_t)ctx->max_smem ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occq, qk->fn, qk->block, smem_seg) !=
+                cudaSuccess ||
+            occq <= 0) {
+            cudaGetLastError();
+            const unsigned seg = s->pair_seg;
+            delete s;
+            SW_SET(ctx, SW_ERR_UNSUPPORTED, "paired shape %dx%d cannot hold a lane of %u rows",
+                   qk->T, qk->R, seg);
+        }
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&s->occ_qp_max, qk->fn, qk->block,
+                                                      qk->smem(qk->T * qk->R));
+        s->qk = qk;
+    }
     const int64_t npairs = ctx->n_pairs;
     s->n_chunks = (int)std::max<int64_t>(1, std::min<int64_t>(o.chunks, std::max<int64_t>(npairs, 1)));
     auto fail = [&](const char* what) {
@@ -529,7 +862,7 @@ extern "C" sw_status sw_serve_start(sw_ctx* ctx, const sw_serve_options* opt) {
          cudaMemcpy(s->d_pair_ids, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess))
         return fail("pair ring");
     if (dev_alloc(&s->d_scores, (size_t)s->n_slots * std::max(n_rec, 1)) != cudaSuccess ||
-        dev_alloc(&s->d_counters, (size_t)s->n_slots + 1) != cudaSuccess)
+        dev_alloc(&s->d_counters, 2 * (size_t)s->n_slots + 2) != cudaSuccess)
         return fail("slots");
     // overflow entries: one per (request, record) at worst, bounded
     s->ovf_cap = std::min<size_t>((size_t)s->n_slots * std::max(n_rec, 1),
@@ -539,12 +872,20 @@ extern "C" sw_status sw_serve_start(sw_ctx* ctx, const sw_serve_options* opt) {
         dev_alloc(&s->d_keys[1], (size_t)s->n_slots * nblk0 * kMaxTopK) != cudaSuccess)
         return fail("key buffers");
     s->bnd_group = 2 * (size_t)std::max(ctx->max_cols, 8);
-    const size_t groups = (size_t)std::max(s->occ_max, 1) * ctx->num_sms * (k->block / k->T);
+    size_t groups = (size_t)std::max(s->occ_max, 1) * ctx->num_sms * (k->block / k->T);
+    if (qk)
+        groups = std::max(groups, (size_t)std::max(s->occ_qp_max, 1) * ctx->num_sms *
+                                      (qk->block / qk->T));
     if (dev_alloc(&s->d_bnd, groups * s->bnd_group) != cudaSuccess) return fail("boundary rows");
-    if (cudaMallocHost((void**)&s->h_keys,
-                       (size_t)s->n_slots * ctx->params.top_k * sizeof(unsigned long long)) !=
-        cudaSuccess)
-        return fail("pinned keys");
+    for (int b = 0; b < 2; ++b) {
+        if (cudaMallocHost((void**)&s->h_keys[b],
+                           (size_t)s->n_slots * ctx->params.top_k * sizeof(unsigned long long)) !=
+                cudaSuccess ||
+            cudaMallocHost((void**)&s->h_flagged[b], sizeof(int)) != cudaSuccess)
+            return fail("pinned keys");
+        if (cudaEventCreateWithFlags(&s->done_ev[b], cudaEventDisableTiming) != cudaSuccess)
+            return fail("round events");
+    }
     s->slots.assign((size_t)s->n_slots, Slot());
     s->stats.slots = (uint32_t)s->n_slots;
     s->stats.chunks = (uint32_t)s->n_chunks;

@@ -126,6 +126,44 @@ __device__ __forceinline__ void forward_cell(uint32_t& Hk, uint32_t& Ek, uint32_
     f = __viaddmax_s16x2(f, K.neg_e2, hq);
 }
 
+// One column step of a thread's two halves: the top half (rows [0, R/2)) on
+// column c with profile words t0/t1, the bottom half (rows [R/2, R)) on column
+// c - 1 with b0/b1.  prev_h / f_in: H and F of the row above the top half
+// (handed down by the thread above, or the boundary row); mid_h / mid_f carry
+// the top half's last row from one column to the bottom half's next; out_h /
+// out_f receive the bottom half's last row (what the thread below takes).
+template <int R, int JSTRIDE>
+__device__ __forceinline__ void column_step(uint32_t (&H)[R], uint32_t (&E)[R],
+                                            const uint2* t0, const uint2* t1,
+                                            const uint2* b0, const uint2* b1,
+                                            uint32_t prev_h, uint32_t f_in,
+                                            uint32_t& mid_h, uint32_t& mid_f,
+                                            uint32_t& out_h, uint32_t& out_f,
+                                            uint32_t& S_top, uint32_t& S_bot,
+                                            const CellK& K) {
+    constexpr int HALF = R / 2;
+    const uint32_t Z = K.bias2;
+    const uint32_t bot_diag = mid_h;
+    uint32_t f_top = f_in, f_bot = mid_f;
+    mid_h = H[HALF - 1];     // the top's last row one column back
+    reverse_sweep<R, 0, HALF>(H, E, t0, t1, JSTRIDE, prev_h);
+    reverse_sweep<R, HALF, R>(H, E, b0, b1, JSTRIDE, bot_diag);
+#pragma unroll
+    for (int i = 0; i < HALF; ++i) {
+        forward_cell(H[i], E[i], f_top, K);
+        forward_cell(H[HALF + i], E[HALF + i], f_bot, K);
+        if (i & 1) S_top = __vimax3_s16x2(S_top, H[i - 1], H[i]);
+        if (i & 1) S_bot = __vimax3_s16x2(S_bot, H[HALF + i - 1], H[HALF + i]);
+        if (!(i & 1) && i == HALF - 1) {
+            S_top = __vimax3_s16x2(S_top, H[i], Z);
+            S_bot = __vimax3_s16x2(S_bot, H[HALF + i], Z);
+        }
+    }
+    mid_f = f_top;
+    out_h = H[R - 1];
+    out_f = f_bot;
+}
+
 // Query profile of one query -> shared memory (whole block; the caller
 // synchronises).  Layout [pass][chunk][code][slot] of 8-byte words holding the
 // signed scores of 8 consecutive rows of the slot's thread.
@@ -166,6 +204,14 @@ struct RunArgs {
     int pair_count;
     int* counter;               // pairs of the range claimed so far
     int P;                      // query passes of T*R rows
+    // A query too long for one launch's profile is scored in row segments by
+    // consecutive launches (plain search only): pass0 = passes of the query
+    // before this launch's first one (that pass reads the boundary row the
+    // previous launch's last pass wrote), more != 0 = a later launch
+    // continues from this launch's last pass (which then writes the boundary
+    // row).  0, 0 for a query that fits one launch.
+    int pass0;
+    int more;
     uint32_t bias2, neg_e;      // see CellK
     uint2* bnd;                 // boundary rows between passes
     size_t bnd_group;           // 0: per-pair rows at bnd + 16*off16; else this many
@@ -187,6 +233,36 @@ struct RunArgs {
 };
 
 
+
+// A record whose first-pass lane may have wrapped, while its query is scored
+// in row segments by several launches: listed once for the 32-bit pass, which
+// overwrites this value with the exact score.
+constexpr int kListed = 0x7fffffff;
+
+// Plain search: a record's first-pass score (biased lane value s) at its
+// sorted position.  A lane that may have wrapped lists the record for the
+// 32-bit pass.  With the query in row segments (pass0 / more) the score is
+// the maximum over the segments, and a listed record keeps kListed so that a
+// later segment does not list it again.
+__device__ __forceinline__ void put_score(const RunArgs& a, int pos, int s, int bias) {
+    if (a.pass0 == 0 && !a.more) {
+        a.scores[pos] = s - bias;
+        if (s >= a.ovf_thresh) {
+            const int j = atomicAdd(a.ovf_count, 1);
+            if (j < a.ovf_cap) a.ovf_list[j] = a.ovf_base + pos;
+        }
+        return;
+    }
+    const int prev = a.scores[pos];
+    if (prev == kListed) return;
+    if (s >= a.ovf_thresh) {
+        a.scores[pos] = kListed;
+        const int j = atomicAdd(a.ovf_count, 1);
+        if (j < a.ovf_cap) a.ovf_list[j] = a.ovf_base + pos;
+    } else {
+        a.scores[pos] = max(prev, s - bias);
+    }
+}
 
 // The group loop: every group of T threads claims pairs from the range and
 // scores them against the query (or query stack) whose profile is in prof;
@@ -253,6 +329,10 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
     uint32_t S_top = Z, S_bot = Z, S_pend = Z, acc_out = Z;
     uint32_t out_h = Z, out_f = Z, prev_h = Z, mid_h = Z, mid_f = Z;
     uint32_t d_bot = kPadPair, d_cur = kPadPair;
+    // the top half's profile offsets of the last column it computed: the
+    // bottom half takes them one step later (its profile base is then the one
+    // the top used, see below)
+    int po0 = kZeroCode * SLOTS, po1 = kZeroCode * SLOTS;
     // the top half's segment
     int pair = 0, pass = 0, ncols = 0, nst = 0, c = 0;
     uint32_t off16 = 0u;
@@ -279,15 +359,19 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
     uint2 bq0 = make_uint2(Z, Z), bq1 = bq0;
     const uint2* rrow = a.bnd;
 
+    // the boundary rows are double-buffered by the parity of the pass's index
+    // in the whole query; a launch's last pass writes one only when a later
+    // launch reads it (that launch starts after this one has finished, so the
+    // 2T + 2 minimum only applies to passes read inside the launch)
 #define SWS_SET_SEG()                                                          \
     {                                                                          \
         const int lo = (pass + 1 < P) ? dep_steps : 3;                         \
         nst = ncols > lo ? ncols : lo;                                         \
         col = reinterpret_cast<const unsigned short*>(a.db) + (size_t)off16 * 8; \
         uint2* const pb = a.bnd_group ? grp_bnd : a.bnd + (size_t)off16 * 16;  \
-        wrow = pb + (pass & 1);                                                \
-        wlim = (pass + 1 < P) ? ncols : 0;                                     \
-        rrow = pb + ((pass - 1) & 1);                                          \
+        wrow = pb + ((a.pass0 + pass) & 1);                                    \
+        wlim = (pass + 1 < P || a.more) ? ncols : 0;                           \
+        rrow = pb + ((a.pass0 + pass - 1) & 1);                                \
         prof_t = prof + pass * PSTRIDE + slot;                                 \
         nload = (pass == 0) ? (nst < 9 ? nst - 1 : 8) : -1;                    \
         if (STACKED) {                                                         \
@@ -318,6 +402,10 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
         b_wlim = wlim;
         c = -2 * t;
         d_cur = (t == 0 && ncols > 0) ? (uint32_t)__ldg(col) : kPadPair;
+        if (t == 0 && a.pass0 > 0) {
+            if (ncols > 0) bq0 = rrow[0];
+            if (ncols > 1) bq1 = rrow[2];
+        }
     }
 
     while (!__all_sync(FULL, fin)) {
@@ -335,7 +423,7 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
         if (t == 0) {
             h_in = Z;
             f_in = Z;
-            if (pass > 0 && c < ncols) {
+            if (a.pass0 + pass > 0 && c < ncols) {
                 h_in = bq0.x;
                 f_in = bq0.y;
                 bq0 = bq1;
@@ -351,29 +439,13 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
         if (!fin && c >= 0) {
             // a column past the segment's end runs on zero-score residues:
             // like a trailing padding column it cannot raise any score
-            const uint2* t0 = prof_t + (int)(d_in & 0xffu) * SLOTS;
-            const uint2* t1 = prof_t + (int)((d_in >> 8) & 0xffu) * SLOTS;
-            const uint2* b0 = prof_b + (int)(d_bot & 0xffu) * SLOTS;
-            const uint2* b1 = prof_b + (int)((d_bot >> 8) & 0xffu) * SLOTS;
-            const uint32_t bot_diag = mid_h;
-            uint32_t f_top = f_in, f_bot = mid_f;
-            mid_h = H[HALF - 1];     // the top's last row one column back
-            reverse_sweep<R, 0, HALF>(H, E, t0, t1, JSTRIDE, prev_h);
-            reverse_sweep<R, HALF, R>(H, E, b0, b1, JSTRIDE, bot_diag);
-#pragma unroll
-            for (int i = 0; i < HALF; ++i) {
-                forward_cell(H[i], E[i], f_top, K);
-                forward_cell(H[HALF + i], E[HALF + i], f_bot, K);
-                if (i & 1) S_top = __vimax3_s16x2(S_top, H[i - 1], H[i]);
-                if (i & 1) S_bot = __vimax3_s16x2(S_bot, H[HALF + i - 1], H[HALF + i]);
-                if (!(i & 1) && i == HALF - 1) {
-                    S_top = __vimax3_s16x2(S_top, H[i], Z);
-                    S_bot = __vimax3_s16x2(S_bot, H[HALF + i], Z);
-                }
-            }
-            mid_f = f_top;
-            out_h = H[R - 1];
-            out_f = f_bot;
+            const int o0 = (int)(d_in & 0xffu) * SLOTS, o1 = (int)((d_in >> 8) & 0xffu) * SLOTS;
+            column_step<R, JSTRIDE>(H, E, prof_t + o0, prof_t + o1,
+                                    prof_b + (int)(d_bot & 0xffu) * SLOTS,
+                                    prof_b + (int)((d_bot >> 8) & 0xffu) * SLOTS, prev_h, f_in,
+                                    mid_h, mid_f, out_h, out_f, S_top, S_bot, K);
+            po0 = o0;
+            po1 = o1;
             if (t == T - 1 && b_col >= 0 && b_col < b_wlim)
                 b_wrow[2 * b_col] = make_uint2(out_h, out_f);
         }
@@ -416,19 +488,8 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
                     acc_out = m;
                     if (t == T - 1) {
                         const int pos = 2 * (a.pair_begin + fpair);
-                        const int s0 = lo16(m), s1 = hi16(m);
-                        a.scores[pos] = s0 - bias;
-                        if (s0 >= a.ovf_thresh) {
-                            const int j = atomicAdd(a.ovf_count, 1);
-                            if (j < a.ovf_cap) a.ovf_list[j] = a.ovf_base + pos;
-                        }
-                        if (pos + 1 < a.n_records) {
-                            a.scores[pos + 1] = s1 - bias;
-                            if (s1 >= a.ovf_thresh) {
-                                const int j = atomicAdd(a.ovf_count, 1);
-                                if (j < a.ovf_cap) a.ovf_list[j] = a.ovf_base + pos + 1;
-                            }
-                        }
+                        put_score(a, pos, lo16(m), bias);
+                        if (pos + 1 < a.n_records) put_score(a, pos + 1, hi16(m), bias);
                     }
                 }
                 S_bot = Z;
@@ -484,7 +545,7 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
                     E[k] = Z;
                 }
                 prev_h = Z;
-                if (t == 0 && pass > 0) {
+                if (t == 0 && a.pass0 + pass > 0) {
                     if (ncols > 0) bq0 = rrow[0];
                     if (ncols > 1) bq1 = rrow[2];
                 }
@@ -492,6 +553,53 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
             }
         }
         ++c;
+
+        // Plain steps: as many steps as every lane of the warp can take with
+        // no segment event (c stays in [1, nst - 2]: no maximum to finish, no
+        // bottom reset, no segment switch), no bounds guard (the residue of
+        // column c + 1 and thread 0's boundary column c + 2 lie inside the
+        // pair) and no pending table-entry load.  In them the bottom half's
+        // profile base and boundary row equal the top's, so the bottom takes
+        // the top's profile offsets of the step before, and the warp runs
+        // without votes or per-step checks.
+        {
+            int k = 0;
+            if (!fin && c >= 1 && !(t == 0 && c <= nload)) {
+                const int last = min(nst - 2, ncols - 3);
+                k = max(last - c + 1, 0);
+            }
+            k = (int)__reduce_min_sync(FULL, (unsigned)k);
+            const bool rd0 = t == 0 && a.pass0 + pass > 0;            // boundary row in
+            const bool zin = (t == 0 && a.pass0 + pass == 0) || (STACKED && my_first);
+            const bool wr = t == T - 1 && wlim > 0;                   // boundary row out
+            for (; k > 0; --k) {
+                if (P > 1) __syncwarp();
+                uint32_t h_in = __shfl_up_sync(FULL, out_h, 1, T);
+                uint32_t f_in = __shfl_up_sync(FULL, out_f, 1, T);
+                const uint32_t d_in = d_cur;
+                d_cur = (uint32_t)__ldg(col + c + 1);
+                if (rd0) {
+                    h_in = bq0.x;
+                    f_in = bq0.y;
+                    bq0 = bq1;
+                    bq1 = rrow[2 * (c + 2)];
+                }
+                if (zin) {
+                    h_in = Z;
+                    f_in = Z;
+                }
+                const int o0 = (int)(d_in & 0xffu) * SLOTS, o1 = (int)((d_in >> 8) & 0xffu) * SLOTS;
+                column_step<R, JSTRIDE>(H, E, prof_t + o0, prof_t + o1, prof_t + po0, prof_t + po1,
+                                        prev_h, f_in, mid_h, mid_f, out_h, out_f, S_top, S_bot, K);
+                if (wr) wrow[2 * (c - 1)] = make_uint2(out_h, out_f);
+                po0 = o0;
+                po1 = o1;
+                prev_h = h_in;
+                d_bot = d_in;
+                b_col = c;
+                ++c;
+            }
+        }
     }
 #undef SWS_SET_SEG
 }
@@ -510,6 +618,8 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_wavefront(const WfArgs a) {
     r.pair_count = a.pair_count;
     r.counter = a.counter;
     r.P = P;
+    r.pass0 = a.pass0;
+    r.more = a.more;
     r.bias2 = a.bias2;
     r.neg_e = a.neg_e;
     r.bnd = a.bnd;
@@ -549,6 +659,8 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_batch(const BatchArgs a) {
         r.pair_count = a.pair_count;
         r.counter = a.counters + i;
         r.P = P;
+        r.pass0 = 0;
+        r.more = 0;
         r.bias2 = a.bias2;
         r.neg_e = a.neg_e;
         r.bnd = a.bnd;

@@ -44,12 +44,15 @@ def mixed():
     return db, qs
 
 
-def test_served_alone_and_mixed_equal_plain(mixed):
+@pytest.mark.parametrize("pair_rows", [None, 0])
+def test_served_alone_and_mixed_equal_plain(mixed, pair_rows):
+    """Default options pair requests of up to 2,048 residues two per register;
+    pair_rows=0 puts every request in stacks."""
     db, qs = mixed
     with capi.Context(0, capi.default_params(top_k=10)) as c:
         c.load_db(db.residues, db.offsets)
         want = [c.search(q)[0] for q in qs]
-        c.serve_start(max_active=64, chunks=3)
+        c.serve_start(max_active=64, chunks=3, pair_rows=pair_rows)
         try:
             # alone: one request at a time
             for i in (0, 6, 12):
@@ -132,7 +135,7 @@ def test_admission_queue_bound_and_errors(mixed):
             with pytest.raises(capi.SwError):
                 c.serve_submit(1, np.zeros(0, dtype=np.uint8))    # empty
             with pytest.raises(capi.SwError):
-                c.serve_submit(1, np.zeros(8193, dtype=np.uint8))  # longer than 8192
+                c.serve_submit(1, np.zeros((1 << 24) + 1, dtype=np.uint8))  # beyond 2^24
             with pytest.raises(capi.SwError):
                 c.serve_submit(1, np.full(10, 25, dtype=np.uint8))  # bad code
             accepted, busy = [], 0
