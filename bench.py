@@ -51,6 +51,10 @@ WORKLOADS = {
     "profile": "profiling case: the full-size DB (~205M residues) and one query of 1,434",
     "stress": "overflow/long-record stress: 100,000 records + 1% of 10,000..40,000 (~58M residues), "
               "0.5% planted homologs, 8 queries 500..4,000, one query per call",
+    "batched": "profiling case: the full-size DB and the 64-query batch (lengths log-uniform "
+               "50..5,000), one sw_search_batch call per step",
+    "traceback": "profiling case: the full-size DB, one query of 1,434 and the alignments of its "
+                 "top-10 hits (sw_traceback) per step",
 }
 
 
@@ -77,6 +81,8 @@ def parse(argv=None):
                     help="skip the overflow / long-record stress measurement")
     ap.add_argument("--kernel-only", action="store_true",
                     help="time the resident path only (no e2e, probe or CPU baseline)")
+    ap.add_argument("--no-pairs", action="store_true",
+                    help="batched profiling case: no paired-query lanes (stacks only)")
     ap.add_argument("--shard", action="store_true",
                     help="one DB split over the ranks (residue-balanced shards, all-gather "
                          "of k hits per query): strong scaling of the sharded search")
@@ -758,8 +764,58 @@ def run_shard(args, rank, world, local_rank, make_ctx=None, workload=None):
             ctx.close()
 
 
+def run_case(args, local_rank):
+    """Profiling cases (--workload batched | traceback): one call of the
+    batched search or of the traceback of a query's hits per step.  Batched:
+    device time by CUDA events inside the library; traceback: host wall time
+    (sw_traceback keeps no device timings).  Prints one JSON line."""
+    import torch
+    from swhybrid_b200 import autotune, capi, synth
+    torch.cuda.set_device(local_rank)
+    db = synth.full_db(2)
+    ctx = capi.Context(local_rank, capi.default_params(top_k=10))
+    try:
+        ctx.load_db(db.residues, db.offsets)
+        autotune.apply(ctx)
+        batched = args.workload == "batched"
+        if batched:
+            if args.no_pairs:        # every query in stacks (the stacked kernel alone)
+                ctx.set_batch_options(pair_rows=0, pair_long=False)
+            qs = synth.batched_queries(3, 64, 50, 5000)
+            cells = sum(len(q) for q in qs) * db.total
+            step = lambda: ctx.search_batch(qs)
+        else:
+            q = synth.query(112, 1434)
+            hits, _ = ctx.search(q)
+            recs = [i for (_, i) in hits]
+            cells = sum(len(q) * len(db.record(int(i))) for i in recs)
+            step = lambda: ctx.traceback(q, recs)
+        for _ in range(args.warmup):
+            step()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        dev = 0.0
+        for _ in range(args.steps):
+            step()
+            if batched:
+                dev += ctx.run_stats().kernel_ms
+        wall = time.perf_counter() - t0
+        if not batched:
+            dev = wall * 1e3
+        print(json.dumps({"workload": WORKLOADS[args.workload], "steps": args.steps,
+                          "ms_per_step_device": round(dev / args.steps, 3),
+                          "ms_per_step_wall": round(wall * 1e3 / args.steps, 3),
+                          "gcups_device": round(cells * args.steps / (dev * 1e-3) / 1e9, 1)
+                          if dev > 0 else None}), flush=True)
+    finally:
+        ctx.close()
+
+
 def main(argv=None):
     args = parse(argv)
+    if args.workload in ("batched", "traceback"):
+        run_case(args, int(os.environ.get("LOCAL_RANK", "0")))
+        return 0
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

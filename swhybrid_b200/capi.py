@@ -141,11 +141,15 @@ class sw_run_stats(ctypes.Structure):
 _lib = None
 
 
-def load(path: str = LIB_PATH):
-    """Load libswb200.so and declare every C-ABI signature."""
+def load(path: str | None = None):
+    """Load libswb200.so and declare every C-ABI signature.  The library
+    built in this package is used unless SWB200_LIBRARY names another build
+    of it (for comparing builds)."""
     global _lib
     if _lib is not None:
         return _lib
+    if path is None:
+        path = os.environ.get("SWB200_LIBRARY") or LIB_PATH
     if not os.path.exists(path):
         raise FileNotFoundError(
             f"{path} is missing: build it with `python -c 'import swhybrid_b200.build as b; b.build()'`")
