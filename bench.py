@@ -308,7 +308,7 @@ def run_reference(args, rank, world):
 
 
 # ---------------------------------------------------------------------------
-def serve_leg(ctx, db, n_req: int, seed: int = 5, levels=(0.25, 0.5, 0.75, 1.0)):
+def serve_leg(ctx, db, n_req: int, seed: int = 5, loads=(0.25, 0.5, 0.75, 1.0)):
     """Serving: requests of lengths log-uniform 30..8,000 (seeded) against the
     resident DB through sw_serve_*.  First the saturating rate (3x the slot
     count submitted at once), then Poisson arrivals at 25/50/75/100% of it,
@@ -344,7 +344,7 @@ def serve_leg(ctx, db, n_req: int, seed: int = 5, levels=(0.25, 0.5, 0.75, 1.0))
         check_ids = []
         base = 1_000_000
         level_qs = requests(n_req)           # the same requests at every offered load
-        for frac in levels:
+        for frac in loads:
             qs = level_qs
             arr = _synth.poisson_arrivals(rng, n_req, frac * sat_rate)
             st0 = ctx.serve_stats()
@@ -386,7 +386,7 @@ def serve_leg(ctx, db, n_req: int, seed: int = 5, levels=(0.25, 0.5, 0.75, 1.0))
         "workload": "requests of lengths log-uniform 30..8,000 (seeded) against the full-size DB; "
                     "saturating rate from %d requests queued at once, then Poisson arrivals at "
                     "%s%% of it, the same %d requests at every level" % (
-                        3 * slots, "/".join(f"{100 * f:g}" for f in levels), n_req),
+                        3 * slots, "/".join(f"{100 * f:g}" for f in loads), n_req),
         "slots": slots, "chunks": int(st.chunks),
         "saturated": {"requests": len(sat_q), "rate_per_s": round(sat_rate, 3),
                       "gcups": round(sat_cells / ((t1 - t0) * 1e-3) / 1e9, 1)},
@@ -599,7 +599,7 @@ def run_ours(args, rank, world, local_rank):
     if args.workload == "full" and args.serve_requests > 0:
         ctx.set_stream(None)
         served = serve_leg(ctx, db, args.serve_requests,
-                           levels=tuple(float(x) for x in args.serve_levels.split(",")))
+                           loads=tuple(float(x) for x in args.serve_levels.split(",")))
 
     # ---- overflow / long-record stress (its own DB and context) ----
     stress = None

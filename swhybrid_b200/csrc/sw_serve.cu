@@ -460,7 +460,7 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
         const int k = ctx->params.top_k;
         const long long nblk0 = std::max<long long>(1, ((long long)n_rec + kTopkKeys - 1) / kTopkKeys);
         long long n = n_rec, in_stride = n_rec;
-        int buf = 0;
+        int kb = 0;                // ping-pong between the two device key buffers
         const unsigned long long* keys_in = nullptr;
         bool first = true;
         while (true) {
@@ -473,7 +473,7 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
             t.k = k;
             t.cap = (ctx->params.flags & SW_FLAG_REFERENCE_CAP) ? 1 : 0;
             t.scores_by_record = nullptr;
-            t.keys_out = s->d_keys[buf];
+            t.keys_out = s->d_keys[kb];
             t.in_stride = in_stride;
             t.rec_stride = 0;
             t.out_stride = nblk0 * kMaxTopK;
@@ -483,9 +483,9 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
                                           dim3((unsigned)blocks, (unsigned)finishing.size()),
                                           dim3(kTopkThreads), args, 0, st));
             ++*launches;
-            keys_in = s->d_keys[buf];
+            keys_in = s->d_keys[kb];
             in_stride = nblk0 * kMaxTopK;
-            buf ^= 1;
+            kb ^= 1;
             first = false;
             if (blocks == 1) break;
             n = blocks * (long long)k;

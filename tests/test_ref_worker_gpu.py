@@ -85,7 +85,8 @@ def test_b200_worker_under_reference_worker_launch(tmp_path):
     want = oracle.search(q, np.concatenate(recs).astype(np.uint8), off, param.blosum62(), 12, 2)
     top = np.sort(want)[::-1][:10]
     assert [int(h[1]) for h in hits] == top.tolist()
-    for h in hits:
-        assert h[3].startswith("r"), h
-        assert want[int(h[3][1:])] == int(h[1]), h
+    for h in hits:                   # DataPool::getTitle gives the header line, '>' included
+        title = h[3].lstrip(">")
+        assert title.startswith("r"), h
+        assert want[int(title[1:])] == int(h[1]), h
     assert top[-1] >= 117      # the hits overflow the reference's int8 pass

@@ -211,16 +211,23 @@ def test_automatic_cutover_on_a_long_tailed_db(ctx, long_case):
         ctx.set_kernel_config(None)
 
 
-def test_refused_search_leaves_nothing_in_flight(ctx, long_case):
-    """A search refused because its query does not fit the shape (with a
-    long-pair split configured) launches nothing, so the next search is exact."""
+def test_segmented_query_and_refused_search(ctx, long_case):
+    """With a long-pair split configured, a query whose profile does not fit
+    one block of the bulk shape (4,097 rows for 4x32) is scored in row
+    segments by consecutive bulk launches beside the long-pair launch; and a
+    search refused before launching (a bad residue code) leaves nothing in
+    flight, so the next search is exact."""
     db, lq, lwant = long_case
     ctx.load_db(db.residues, db.offsets)
     try:
         ctx.set_kernel_config((32, 16, 4, 32, 1500))
+        _, scores = ctx.search(lq[3], want_scores=True)
+        np.testing.assert_array_equal(scores, lwant[3])
+        bad = lq[1].copy()
+        bad[5] = 25
         with pytest.raises(capi.SwError) as e:
-            ctx.search(lq[3])                      # 4,097 rows: too big for 4x32
-        assert e.value.status == 6
+            ctx.search(bad)
+        assert e.value.status == 1
         _, scores = ctx.search(lq[0], want_scores=True)
         np.testing.assert_array_equal(scores, lwant[0])
     finally:
