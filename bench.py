@@ -55,6 +55,7 @@ WORKLOADS = {
                "50..5,000), one sw_search_batch call per step",
     "traceback": "profiling case: the full-size DB, one query of 1,434 and the alignments of its "
                  "top-10 hits (sw_traceback) per step",
+    "probe": "the roofline probe alone: register-only cell mixes and issue rates (libswprobe.so)",
 }
 
 
@@ -815,6 +816,9 @@ def main(argv=None):
     args = parse(argv)
     if args.workload in ("batched", "traceback"):
         run_case(args, int(os.environ.get("LOCAL_RANK", "0")))
+        return 0
+    if args.workload == "probe":
+        print(json.dumps(probe_rates(int(os.environ.get("LOCAL_RANK", "0")))), flush=True)
         return 0
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
