@@ -399,11 +399,13 @@ typedef struct sw_serve_options {
                                  shape pair_group_width x pair_rows_per_thread; 0 = off */
     int32_t pair_group_width;
     int32_t pair_rows_per_thread;
+    int32_t pair_long;        /* != 0: longer requests are paired too (a lane each, scored
+                                 in pair_rows-row segments by consecutive launches) */
 } sw_serve_options;
 
 /* Defaults: 128 slots, 4 chunks, unbounded queue, half the free memory,
- * shape 16x64, stacks of 4096 rows, requests of up to 2048 residues paired
- * two per register with shape 16x64 (as sw_search_batch does). */
+ * shape 16x64, stacks of 4096 rows, every request paired two per register
+ * with shape 16x64, in lanes of up to 2048 rows (as sw_search_batch does). */
 void sw_serve_options_default(sw_serve_options *opt);
 
 typedef struct sw_serve_result {

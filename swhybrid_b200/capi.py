@@ -94,7 +94,8 @@ class sw_serve_options(ctypes.Structure):
                 ("max_pending", ctypes.c_uint32), ("memory_budget", ctypes.c_uint64),
                 ("group_width", ctypes.c_int32), ("rows_per_thread", ctypes.c_int32),
                 ("stack_rows", ctypes.c_int32), ("pair_rows", ctypes.c_int32),
-                ("pair_group_width", ctypes.c_int32), ("pair_rows_per_thread", ctypes.c_int32)]
+                ("pair_group_width", ctypes.c_int32), ("pair_rows_per_thread", ctypes.c_int32),
+                ("pair_long", ctypes.c_int32)]
 
 
 class sw_serve_result(ctypes.Structure):
@@ -514,7 +515,8 @@ class Context:
 
     # ---- serving ----------------------------------------------------------
     def serve_start(self, max_active=None, chunks=None, max_pending=None, memory_budget=None,
-                    shape=None, stack_rows=None, pair_rows=None, pair_shape=None):
+                    shape=None, stack_rows=None, pair_rows=None, pair_shape=None,
+                    pair_long=None):
         o = sw_serve_options()
         self.L.sw_serve_options_default(ctypes.byref(o))
         if max_active is not None:
@@ -533,6 +535,8 @@ class Context:
             o.pair_rows = pair_rows
         if pair_shape is not None:
             o.pair_group_width, o.pair_rows_per_thread = pair_shape
+        if pair_long is not None:
+            o.pair_long = 1 if pair_long else 0
         self._check(self.L.sw_serve_start(self.h, ctypes.byref(o)), "sw_serve_start")
 
     def serve_submit(self, request_id: int, query: np.ndarray) -> int:

@@ -93,7 +93,8 @@ struct sw_serve_state {
     int* d_scores = nullptr;              // [slot][sorted position]
     uint8_t* d_meta = nullptr;            // per-round tables (layout in run_round)
     size_t meta_cap = 0;
-    int* d_counters = nullptr;            // one per stack, overflow count last
+    int* d_counters = nullptr;            // stacks, the overflow count, paired launch entries
+    size_t counters_cap = 0;
     int* d_ovf = nullptr;
     size_t ovf_cap = 0;
     uint2* d_bnd = nullptr;
@@ -169,10 +170,13 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
     // one record (sw_qpbatch, packed profile); the others: stacks
     const QpKernel* qk = s->qk;
     const uint32_t qR = qk ? (uint32_t)qk->R : 1u, qT = qk ? (uint32_t)qk->T : 1u;
+    // (with pair_long every request: one longer than a lane gets a lane of
+    // its own, scored in lane-height segments by consecutive launches)
     std::vector<int> paired, stacked;
     for (int sl : active) {
         const uint32_t L = (uint32_t)s->slots[sl].req.query.size();
-        (qk && (L + qR - 1) / qR * qR <= s->pair_seg ? paired : stacked).push_back(sl);
+        const bool fits = (L + qR - 1) / qR * qR <= s->pair_seg;
+        (qk && (fits || s->opt.pair_long) ? paired : stacked).push_back(sl);
     }
     struct Stack {
         std::vector<int> slots;
@@ -252,15 +256,25 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
     }
     if (lanes.size() % 2) lanes.push_back(Lane{});
     const size_t nd = lanes.size() / 2;
-    std::vector<uint32_t> qp_off[2], qp_rows[2], qp_rboff;
+    // entries of the paired launches: one per (double stack, segment); every
+    // single-segment double stack in the first launch, then each taller one's
+    // segments in launches of their own, one after another (segment s reads
+    // the rows above from segment s-1 through the per-record boundary rows)
+    std::vector<uint32_t> qp_off[2], qp_rows[2], qp_rboff, qp_flags;
     std::vector<int32_t> qp_rbmap;           // (low, high) entries
-    uint32_t qp_max_rows = 0;
+    struct QpLaunch {
+        size_t first = 0, count = 0;
+        uint32_t max_rows = 0;
+    };
+    std::vector<QpLaunch> qp_launches;
+    std::vector<uint32_t> d_off[2];
+    std::vector<std::vector<int32_t>> d_blocks[2];
+    std::vector<uint32_t> d_nseg;
     for (size_t d = 0; d < nd; ++d) {
-        std::vector<int32_t> blocks[2];
         for (int h = 0; h < 2; ++h) {
             const Lane& ln = lanes[2 * d + h];
-            qp_off[h].push_back((uint32_t)codes.size());
-            qp_rows[h].push_back(ln.rows);
+            d_off[h].push_back((uint32_t)codes.size());
+            d_blocks[h].emplace_back();
             for (int sl : ln.slots) {
                 const std::vector<uint8_t>& q = s->slots[sl].req.query;
                 const uint32_t L = (uint32_t)q.size();
@@ -270,17 +284,47 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
                 codes.insert(codes.end(), q.begin(), q.end());
                 codes.insert(codes.end(), padded - L, (uint8_t)kZeroCode);
                 for (uint32_t j = 0; j < padded / qR; ++j)
-                    blocks[h].push_back((int32_t)sl | (j == 0 ? kFirstBit : 0));
+                    d_blocks[h].back().push_back((int32_t)sl | (j == 0 ? kFirstBit : 0));
             }
         }
         const uint32_t rows = std::max(lanes[2 * d].rows, lanes[2 * d + 1].rows);
-        qp_max_rows = std::max(qp_max_rows, rows);
+        d_nseg.push_back(std::max<uint32_t>(1, (rows + s->pair_seg - 1) / s->pair_seg));
+    }
+    auto add_entry = [&](size_t d, uint32_t lv) {
+        uint32_t rs[2];
+        for (int h = 0; h < 2; ++h) {
+            const uint32_t lr = lanes[2 * d + h].rows;
+            rs[h] = lr > lv * s->pair_seg ? std::min(s->pair_seg, lr - lv * s->pair_seg) : 0u;
+            qp_off[h].push_back(d_off[h][d] + lv * s->pair_seg);
+            qp_rows[h].push_back(rs[h]);
+        }
+        const uint32_t rows = std::max(rs[0], rs[1]);
         const uint32_t P = std::max<uint32_t>(1, (rows + qT * qR - 1) / (qT * qR));
         qp_rboff.push_back((uint32_t)(qp_rbmap.size() / 2));
+        qp_flags.push_back((lv > 0 ? 1u : 0u) | (lv + 1 < d_nseg[d] ? 2u : 0u));
+        const size_t b0 = (size_t)lv * s->pair_seg / qR;
         for (uint32_t j = 0; j < P * qT; ++j)
             for (int h = 0; h < 2; ++h)
-                qp_rbmap.push_back(j < blocks[h].size() ? blocks[h][j] : -1);
+                qp_rbmap.push_back(b0 + j < d_blocks[h][d].size() ? d_blocks[h][d][b0 + j] : -1);
+        return rows;
+    };
+    {
+        QpLaunch L0;
+        L0.first = qp_flags.size();
+        for (size_t d = 0; d < nd; ++d)
+            if (d_nseg[d] == 1) L0.max_rows = std::max(L0.max_rows, add_entry(d, 0));
+        L0.count = qp_flags.size() - L0.first;
+        if (L0.count) qp_launches.push_back(L0);
+        for (size_t d = 0; d < nd; ++d)
+            for (uint32_t lv = 0; d_nseg[d] > 1 && lv < d_nseg[d]; ++lv) {
+                QpLaunch Ls;
+                Ls.first = qp_flags.size();
+                Ls.max_rows = add_entry(d, lv);
+                Ls.count = 1;
+                qp_launches.push_back(Ls);
+            }
     }
+    const size_t ne = qp_flags.size();
     // table layout (one upload; the paired block map is read as int2)
     size_t total = 0;
     auto place = [&total](size_t bytes, size_t align) {
@@ -292,8 +336,9 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
     const size_t o_soff = place(4 * ns, 4), o_srows = place(4 * ns, 4), o_rboff = place(4 * ns, 4);
     const size_t o_rbmap = place(4 * rbmap.size(), 4);
     const size_t o_rows = place(4 * finishing.size(), 4);
-    const size_t o_qpo0 = place(4 * nd, 4), o_qpr0 = place(4 * nd, 4);
-    const size_t o_qpo1 = place(4 * nd, 4), o_qpr1 = place(4 * nd, 4), o_qprb = place(4 * nd, 4);
+    const size_t o_qpo0 = place(4 * ne, 4), o_qpr0 = place(4 * ne, 4);
+    const size_t o_qpo1 = place(4 * ne, 4), o_qpr1 = place(4 * ne, 4), o_qprb = place(4 * ne, 4);
+    const size_t o_qpfl = place(4 * ne, 4);
     const size_t o_qpmap = place(4 * qp_rbmap.size(), 8);
     const size_t o_codes = place(codes.size(), 16);
     total = (total + 15) / 16 * 16;
@@ -326,12 +371,13 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
         memcpy(m + o_rbmap, rbmap.data(), 4 * rbmap.size());
     }
     if (!finishing.empty()) memcpy(m + o_rows, finishing.data(), 4 * finishing.size());
-    if (nd) {
-        memcpy(m + o_qpo0, qp_off[0].data(), 4 * nd);
-        memcpy(m + o_qpr0, qp_rows[0].data(), 4 * nd);
-        memcpy(m + o_qpo1, qp_off[1].data(), 4 * nd);
-        memcpy(m + o_qpr1, qp_rows[1].data(), 4 * nd);
-        memcpy(m + o_qprb, qp_rboff.data(), 4 * nd);
+    if (ne) {
+        memcpy(m + o_qpo0, qp_off[0].data(), 4 * ne);
+        memcpy(m + o_qpr0, qp_rows[0].data(), 4 * ne);
+        memcpy(m + o_qpo1, qp_off[1].data(), 4 * ne);
+        memcpy(m + o_qpr1, qp_rows[1].data(), 4 * ne);
+        memcpy(m + o_qprb, qp_rboff.data(), 4 * ne);
+        memcpy(m + o_qpfl, qp_flags.data(), 4 * ne);
         memcpy(m + o_qpmap, qp_rbmap.data(), 4 * qp_rbmap.size());
     }
     if (!codes.empty()) memcpy(m + o_codes, codes.data(), codes.size());
@@ -341,17 +387,20 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
         if (s->slots[sl].fresh)
             SW_CUDA(ctx, cudaMemsetAsync(s->d_scores + (size_t)sl * n_rec, 0,
                                          (size_t)n_rec * sizeof(int), st));
-    // counters: stack i at [i], the overflow count at [ns], double stack j at
+    // counters: stack i at [i], the overflow count at [ns], paired entry j at
     // [ns + 1 + j]
-    SW_CUDA(ctx, cudaMemsetAsync(s->d_counters, 0, (ns + 1 + nd) * sizeof(int), st));
+    if (ns + 1 + ne > s->counters_cap)
+        SW_SET(ctx, SW_ERR_UNSUPPORTED, "%zu paired launch entries exceed the counters (%zu)", ne,
+               s->counters_cap);
+    SW_CUDA(ctx, cudaMemsetAsync(s->d_counters, 0, (ns + 1 + ne) * sizeof(int), st));
     const int occ = ns ? std::min(shape_occupancy(ctx, *s->k, (int)max_rows), s->occ_max) : 1;
     if (occ <= 0)
         SW_SET(ctx, SW_ERR_UNSUPPORTED, "a stack of %u rows does not fit shape %dx%d", max_rows,
                T, R);
     int* d_ovf_count = s->d_counters + ns;
     const int pair_count = s->chunk_begin[chunk + 1] - s->chunk_begin[chunk];
-    if (nd && pair_count > 0) {
-        const size_t smem = qk->smem((int)std::max<uint32_t>(qp_max_rows, 1));
+    for (const QpLaunch& L : pair_count > 0 ? qp_launches : std::vector<QpLaunch>()) {
+        const size_t smem = qk->smem((int)std::max<uint32_t>(L.max_rows, 1));
         int occq = 0;
         if (smem > (size_t)ctx->max_smem ||
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occq, qk->fn, qk->block, smem) !=
@@ -362,21 +411,22 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
         occq = std::min(occq, s->occ_qp_max);
         if (occq <= 0)
             SW_SET(ctx, SW_ERR_UNSUPPORTED, "paired lanes of %u rows do not fit shape %dx%d",
-                   qp_max_rows, qk->T, qk->R);
+                   L.max_rows, qk->T, qk->R);
+        const uint32_t* base = reinterpret_cast<const uint32_t*>(s->d_meta);
         QpArgs q;
         q.db = ctx->d_db;
         q.pairs = s->d_pairs;
         q.pair_begin = s->chunk_begin[chunk];
         q.pair_count = pair_count;
         q.codes = s->d_meta + o_codes;
-        q.off_lo = reinterpret_cast<const uint32_t*>(s->d_meta + o_qpo0);
-        q.rows_lo = reinterpret_cast<const uint32_t*>(s->d_meta + o_qpr0);
-        q.off_hi = reinterpret_cast<const uint32_t*>(s->d_meta + o_qpo1);
-        q.rows_hi = reinterpret_cast<const uint32_t*>(s->d_meta + o_qpr1);
+        q.off_lo = base + o_qpo0 / 4 + L.first;
+        q.rows_lo = base + o_qpr0 / 4 + L.first;
+        q.off_hi = base + o_qpo1 / 4 + L.first;
+        q.rows_hi = base + o_qpr1 / 4 + L.first;
         q.rb_map = reinterpret_cast<const int2*>(s->d_meta + o_qpmap);
-        q.rb_off = reinterpret_cast<const uint32_t*>(s->d_meta + o_qprb);
-        q.nstacks = (int)nd;
-        q.counters = s->d_counters + ns + 1;
+        q.rb_off = base + o_qprb / 4 + L.first;
+        q.nstacks = (int)L.count;
+        q.counters = s->d_counters + ns + 1 + L.first;
         q.mat = ctx->d_mat;
         q.bias2 = (uint32_t)(ctx->params.gap_open + ctx->params.gap_extend);
         q.bias2 |= q.bias2 << 16;
@@ -391,8 +441,11 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
         q.ovf_thresh = 32767 - std::max(ctx->max_score, 1) + 1;
         q.ovf_cap = (int)std::min<size_t>(s->ovf_cap, (size_t)INT32_MAX);
         q.pair_ids = s->d_pair_ids;
-        q.seg_flags = nullptr;       // a paired lane is never cut into segments here
-        q.seg_bnd = s->d_bnd;
+        q.seg_flags = base + o_qpfl / 4 + L.first;
+        // a segment's last row for the next segment: the context's per-record
+        // boundary rows (the plain search's; it does not run while a round is
+        // on the stream)
+        q.seg_bnd = ctx->d_bnd;
         void* qargs[] = {&q};
         SW_CUDA(ctx, cudaLaunchKernel(qk->fn, dim3((unsigned)(occq * ctx->num_sms)),
                                       dim3(qk->block), qargs, smem, st));
@@ -766,6 +819,7 @@ extern "C" void sw_serve_options_default(sw_serve_options* o) {
     o->pair_rows = 2048;
     o->pair_group_width = 16;
     o->pair_rows_per_thread = 64;
+    o->pair_long = 1;
 }
 
 extern "C" sw_status sw_serve_start(sw_ctx* ctx, const sw_serve_options* opt) {
@@ -862,7 +916,7 @@ extern "C" sw_status sw_serve_start(sw_ctx* ctx, const sw_serve_options* opt) {
          cudaMemcpy(s->d_pair_ids, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess))
         return fail("pair ring");
     if (dev_alloc(&s->d_scores, (size_t)s->n_slots * std::max(n_rec, 1)) != cudaSuccess ||
-        dev_alloc(&s->d_counters, 2 * (size_t)s->n_slots + 2) != cudaSuccess)
+        dev_alloc(&s->d_counters, 4 * (size_t)s->n_slots + 8) != cudaSuccess)
         return fail("slots");
     // overflow entries: one per (request, record) at worst, bounded
     s->ovf_cap = std::min<size_t>((size_t)s->n_slots * std::max(n_rec, 1),
@@ -886,6 +940,10 @@ extern "C" sw_status sw_serve_start(sw_ctx* ctx, const sw_serve_options* opt) {
         if (cudaEventCreateWithFlags(&s->done_ev[b], cudaEventDisableTiming) != cudaSuccess)
             return fail("round events");
     }
+    // stacks (at most one per slot), the overflow count, and paired entries
+    // (a lane of at most max_stack_rows rows has at most that / pair_seg
+    // segments; two lanes per double stack)
+    s->counters_cap = 4 * (size_t)s->n_slots + 8;
     s->slots.assign((size_t)s->n_slots, Slot());
     s->stats.slots = (uint32_t)s->n_slots;
     s->stats.chunks = (uint32_t)s->n_chunks;

@@ -572,6 +572,8 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
             const bool rd0 = t == 0 && a.pass0 + pass > 0;            // boundary row in
             const bool zin = (t == 0 && a.pass0 + pass == 0) || (STACKED && my_first);
             const bool wr = t == T - 1 && wlim > 0;                   // boundary row out
+            // two steps per iteration (+0.9 % over the sweep, measured)
+#pragma unroll 2
             for (; k > 0; --k) {
                 if (P > 1) __syncwarp();
                 uint32_t h_in = __shfl_up_sync(FULL, out_h, 1, T);

@@ -44,15 +44,16 @@ def mixed():
     return db, qs
 
 
-@pytest.mark.parametrize("pair_rows", [None, 0])
-def test_served_alone_and_mixed_equal_plain(mixed, pair_rows):
-    """Default options pair requests of up to 2,048 residues two per register;
-    pair_rows=0 puts every request in stacks."""
+@pytest.mark.parametrize("opts", [{}, {"pair_long": False}, {"pair_rows": 0}])
+def test_served_alone_and_mixed_equal_plain(mixed, opts):
+    """Default options pair every request two per register (requests longer
+    than a 2,048-row lane in segments by consecutive launches); pair_long off
+    pairs only the short ones and stacks the rest; pair_rows=0 stacks all."""
     db, qs = mixed
     with capi.Context(0, capi.default_params(top_k=10)) as c:
         c.load_db(db.residues, db.offsets)
         want = [c.search(q)[0] for q in qs]
-        c.serve_start(max_active=64, chunks=3, pair_rows=pair_rows)
+        c.serve_start(max_active=64, chunks=3, **opts)
         try:
             # alone: one request at a time
             for i in (0, 6, 12):
