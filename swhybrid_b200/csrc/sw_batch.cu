@@ -19,6 +19,7 @@
 // The whole sequence (query upload, launches, result download) is captured
 // once per batch signature and replayed.
 #include <algorithm>
+#include <array>
 #include <chrono>
 #include <cstring>
 #include <map>
@@ -56,6 +57,7 @@ struct StackPlan {
     // double stacks of the paired-query kernel: per double stack the two lanes'
     // codes offset and rows, and per (pass, thread) the (low, high) block map
     std::vector<uint32_t> qp_off_lo, qp_rows_lo, qp_off_hi, qp_rows_hi, qp_rb_off, qp_flags;
+    std::vector<uint32_t> qp_slot;        // boundary region of each segmented entry
     std::vector<int32_t> qp_rb_map;       // pairs of entries
 };
 
@@ -91,6 +93,11 @@ struct sw_batch_state {
     size_t keys_cap = 0;
     uint2* d_bnd = nullptr;
     size_t bnd_cap = 0;
+    // boundary regions of tall paired double stacks whose segments share a
+    // launch (one per stack of a wave; 1 = the context's own rows, d_segbnd unused)
+    uint2* d_segbnd = nullptr;
+    int seg_regions = 1;
+    size_t seg_stride = 0;         // entries per region
     // pinned host staging
     uint8_t* h_stage = nullptr;      // queries, then meta
     size_t stage_cap = 0;
@@ -117,6 +124,7 @@ void free_batch(sw_ctx* ctx) {
     dev_free(b->d_keys[0]);
     dev_free(b->d_keys[1]);
     dev_free(b->d_bnd);
+    dev_free(b->d_segbnd);
     if (b->h_stage) cudaFreeHost(b->h_stage);
     if (b->h_keys) cudaFreeHost(b->h_keys);
     delete b;
@@ -143,17 +151,65 @@ double wall_ms() {
         .count();
 }
 
+// Boundary regions for `want` tall double stacks whose segments share
+// launches: at most 4, as many as fit in a quarter of the free device memory
+// (each is a copy of the context's per-record boundary rows, 8 bytes per
+// column of every record); 1 means the context's own rows.  Grows (never
+// shrinks) the batch state's region buffer; called before any capture.
+int seg_regions_for(sw_ctx* ctx, sw_batch_state* b, int want) {
+    const size_t stride = (size_t)ctx->db_units * 16;
+    if (b->d_segbnd && b->seg_stride != stride) {   // sized for another DB
+        for (auto& kv : b->graphs) {
+            if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+            if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+        }
+        b->graphs.clear();
+        dev_free(b->d_segbnd);
+        b->d_segbnd = nullptr;
+        b->seg_regions = 1;
+        b->seg_stride = 0;
+    }
+    want = std::max(1, std::min(want, 4));
+    if (want <= 1 || stride == 0) return 1;
+    if (b->seg_regions >= want && b->seg_stride == stride) return want;
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        return b->seg_stride == stride ? b->seg_regions : 1;
+    }
+    const size_t held = b->seg_stride == stride && b->d_segbnd ? (size_t)b->seg_regions : 0;
+    const size_t fit = (free_b / 4 + held * stride * sizeof(uint2)) / (stride * sizeof(uint2));
+    const int n = (int)std::min<size_t>((size_t)want, fit);
+    if (n <= 1) return b->seg_stride == stride && b->d_segbnd ? b->seg_regions : 1;
+    for (auto& kv : b->graphs) {      // graphs hold the old pointer
+        if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+        if (kv.second.graph) cudaGraphDestroy(kv.second.graph);
+    }
+    b->graphs.clear();
+    dev_free(b->d_segbnd);
+    b->seg_regions = 1;
+    b->seg_stride = 0;
+    if (dev_alloc(&b->d_segbnd, (size_t)n * stride) != cudaSuccess) {
+        cudaGetLastError();
+        b->d_segbnd = nullptr;
+        return 1;
+    }
+    b->seg_regions = n;
+    b->seg_stride = stride;
+    return n;
+}
+
 // Enqueues one batch on ctx->stream (and the side stream).  Buffers are sized.
 // Device layout of d_meta (and of the staging area it is copied from):
 //   qoff[nq], qlen[nq]                          uint32
 //   stack_off[ns], stack_rows[ns], rb_off[ns]   uint32
 //   rb_map[...]                                 int32
 //   stack codes                                 uint8
-//   qp_off_lo, qp_rows_lo, qp_off_hi, qp_rows_hi, qp_rb_off [nqp]  uint32
+//   qp_off_lo, qp_rows_lo, qp_off_hi, qp_rows_hi, qp_rb_off, qp_flags, qp_slot [nqp]  uint32
 //   qp_rb_map[...] (16-byte aligned)            int2
 struct MetaLayout {
     size_t qoff, qlen, soff, srows, rboff, rbmap, qp_off_lo, qp_rows_lo, qp_off_hi, qp_rows_hi,
-        qp_rboff, qp_flags, qp_rbmap, codes, total;
+        qp_rboff, qp_flags, qp_slot, qp_rbmap, codes, total;
     int nst, nqp;
 };
 
@@ -174,7 +230,8 @@ MetaLayout meta_layout(uint32_t nq, const StackPlan& sp) {
     m.qp_rows_hi = m.qp_off_hi + 4 * nqp;
     m.qp_rboff = m.qp_rows_hi + 4 * nqp;
     m.qp_flags = m.qp_rboff + 4 * nqp;
-    m.qp_rbmap = (m.qp_flags + 4 * nqp + 15) / 16 * 16;
+    m.qp_slot = m.qp_flags + 4 * nqp;
+    m.qp_rbmap = (m.qp_slot + 4 * nqp + 15) / 16 * 16;
     m.codes = m.qp_rbmap + 4 * sp.qp_rb_map.size();
     m.total = (m.codes + sp.codes.size() + 15) / 16 * 16;
     return m;
@@ -237,7 +294,9 @@ sw_status enqueue_batch(sw_ctx* ctx, sw_batch_state* b, uint32_t nq, size_t qbyt
             q.ovf_cap = (int)std::min<size_t>(b->ovf_cap, (size_t)INT32_MAX);
             q.pair_ids = nullptr;
             q.seg_flags = reinterpret_cast<const uint32_t*>(b->d_meta + ml.qp_flags) + L.sbegin;
-            q.seg_bnd = ctx->d_bnd;
+            q.seg_bnd = b->d_segbnd ? b->d_segbnd : ctx->d_bnd;
+            q.seg_slot = reinterpret_cast<const uint32_t*>(b->d_meta + ml.qp_slot) + L.sbegin;
+            q.seg_stride = b->seg_stride;
             void* args[] = {&q};
             SW_CUDA(ctx, cudaLaunchKernel(L.qk->fn, dim3((unsigned)L.grid), dim3(L.threads), args,
                                           L.smem, st));
@@ -604,22 +663,39 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
             }
             D.nseg = std::max<uint32_t>(1, (std::max(D.rows[0], D.rows[1]) + seg - 1) / seg);
         }
-        // launches: every single-segment double stack in one launch; then each
-        // taller double stack's segments in launches of their own, one after
-        // another (they share the per-record boundary buffer)
-        std::vector<std::vector<std::pair<size_t, uint32_t>>> groups(1);   // (double stack, segment)
+        // launches: every single-segment double stack in one launch; then the
+        // taller double stacks in waves of as many as there are boundary
+        // regions (each stack of a wave hands its segments' last rows on
+        // through a region of its own): per wave, one launch per segment
+        // level with every stack of the wave that has that segment, the levels
+        // one after another
+        std::vector<size_t> tall;
         for (size_t d = 0; d < dbl.size(); ++d)
-            if (dbl[d].nseg == 1) groups[0].push_back({d, 0u});
+            if (dbl[d].nseg > 1) tall.push_back(d);
+        const int regions = seg_regions_for(ctx, b, (int)tall.size());
+        // (double stack, segment, region)
+        std::vector<std::vector<std::array<uint32_t, 3>>> groups(1);
         for (size_t d = 0; d < dbl.size(); ++d)
-            for (uint32_t lv = 0; dbl[d].nseg > 1 && lv < dbl[d].nseg; ++lv)
-                groups.push_back({{d, lv}});
+            if (dbl[d].nseg == 1) groups[0].push_back({(uint32_t)d, 0u, 0u});
+        for (size_t w0 = 0; w0 < tall.size(); w0 += (size_t)regions) {
+            const size_t w1 = std::min(tall.size(), w0 + (size_t)regions);
+            uint32_t levels = 0;
+            for (size_t i = w0; i < w1; ++i) levels = std::max(levels, dbl[tall[i]].nseg);
+            for (uint32_t lv = 0; lv < levels; ++lv) {
+                groups.emplace_back();
+                for (size_t i = w0; i < w1; ++i)
+                    if (lv < dbl[tall[i]].nseg)
+                        groups.back().push_back({(uint32_t)tall[i], lv, (uint32_t)(i - w0)});
+            }
+        }
         for (const auto& grp : groups) {
             if (grp.empty()) continue;
             const int first = (int)sp.qp_off_lo.size();
             uint32_t max_rows = 0;
             for (const auto& e : grp) {
-                const Double& D = dbl[e.first];
-                const uint32_t lv = e.second;
+                const Double& D = dbl[e[0]];
+                const uint32_t lv = e[1];
+                sp.qp_slot.push_back(e[2]);
                 uint32_t rs[2];
                 for (int h = 0; h < 2; ++h) {
                     rs[h] = D.rows[h] > lv * seg ? std::min(seg, D.rows[h] - lv * seg) : 0u;
@@ -761,6 +837,7 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
         memcpy(m + ml.qp_rows_hi, sp.qp_rows_hi.data(), 4 * nqp);
         memcpy(m + ml.qp_rboff, sp.qp_rb_off.data(), 4 * nqp);
         memcpy(m + ml.qp_flags, sp.qp_flags.data(), 4 * nqp);
+        memcpy(m + ml.qp_slot, sp.qp_slot.data(), 4 * nqp);
         memcpy(m + ml.qp_rbmap, sp.qp_rb_map.data(), 4 * sp.qp_rb_map.size());
         memcpy(m + ml.codes, sp.codes.data(), sp.codes.size());
     }

@@ -398,6 +398,7 @@ sw_status swb::db_load(sw_ctx* ctx, const uint8_t* residues, const uint64_t* off
     if (dev_alloc(&ctx->d_pairs, npairs_all) != cudaSuccess) return nomem("pairs");
     if (dev_alloc(&ctx->d_perm, n) != cudaSuccess) return nomem("perm");
     if (dev_alloc(&ctx->d_bnd, units * 16) != cudaSuccess) return nomem("boundary rows");
+    ctx->db_units = (uint64_t)units;
     if (dev_alloc(&ctx->d_scores, n + 1) != cudaSuccess) return nomem("scores");
     if (dev_alloc(&ctx->d_scores_rec, n + 1) != cudaSuccess) return nomem("scores");
     if (dev_alloc(&ctx->d_ovf, n + 1) != cudaSuccess) return nomem("overflow list");

@@ -88,6 +88,7 @@ struct sw_ctx {
     swb::Pair2* d_pairs = nullptr;
     uint32_t* d_perm = nullptr;        // sorted position -> record
     uint2* d_bnd = nullptr;            // boundary rows between query passes
+    uint64_t db_units = 0;             // 16-byte units of the column streams (d_bnd: 16 each)
     int* d_scores = nullptr;           // per sorted position
     int* d_scores_rec = nullptr;       // per record
     int* d_ovf = nullptr;              // overflow list

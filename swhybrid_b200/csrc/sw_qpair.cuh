@@ -58,6 +58,10 @@ struct QpArgs {
     const uint32_t* seg_flags;
     uint2* seg_bnd;             // per record and column: (H, F) of a segment's last row,
                                 // at 16 entries per 16-byte stream unit (2 per column)
+    // several tall double stacks' segments in one launch: stack i uses the
+    // boundary region seg_bnd + seg_slot[i] * seg_stride (null: region 0)
+    const uint32_t* seg_slot;
+    size_t seg_stride;
 };
 
 // Shared-memory bytes of a double stack's profile (rows = the taller lane).
@@ -167,7 +171,7 @@ __device__ __forceinline__ void column_step_qp(uint32_t (&H)[R], uint32_t (&E)[R
 // pass's thread T-1 writes it, so one buffer serves both.
 template <int T, int R>
 __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, int P, int* counter,
-                                           const int2* rb_map, uint32_t seg) {
+                                           const int2* rb_map, uint32_t seg, size_t seg_base) {
     static_assert(R % 8 == 0, "R");
     constexpr int NJ = R / 4;
     constexpr int HALF = R / 2;
@@ -228,7 +232,7 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
         const int lo = (pass + 1 < P) ? dep_steps : 3;                         \
         nst = ncols > lo ? ncols : lo;                                         \
         col = reinterpret_cast<const unsigned short*>(a.db) + (size_t)off16 * 8; \
-        uint2* const sb = a.seg_bnd + (size_t)off16 * 16 + half;               \
+        uint2* const sb = a.seg_bnd + seg_base + (size_t)off16 * 16 + half;    \
         wrow = (pass + 1 < P) ? pbnd + (pass & 1) : sb;                        \
         wlim = (pass + 1 < P || (seg & 2u)) ? ncols : 0;                       \
         has_in = pass > 0 || (seg & 1u);                                       \
@@ -458,7 +462,8 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_qpbatch(const QpArgs a) {
                                a.codes + a.off_hi[i], (int)a.rows_hi[i], a.mat, P);
         __syncthreads();
         run_qpairs<T, R>(a, prof4, P, a.counters + i, a.rb_map + a.rb_off[i],
-                         a.seg_flags ? a.seg_flags[i] : 0u);
+                         a.seg_flags ? a.seg_flags[i] : 0u,
+                         a.seg_slot ? (size_t)a.seg_slot[i] * a.seg_stride : (size_t)0);
     }
 }
 

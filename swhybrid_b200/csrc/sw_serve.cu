@@ -99,6 +99,9 @@ struct sw_serve_state {
     size_t ovf_cap = 0;
     uint2* d_bnd = nullptr;
     size_t bnd_group = 0;
+    uint2* d_segbnd = nullptr;            // boundary regions of tall paired double stacks
+    int seg_regions = 1;                  // (1: the context's own rows, d_segbnd null)
+    size_t seg_stride = 0;
     unsigned long long* d_keys[2] = {nullptr, nullptr};
     // per-round host buffers, two sets: round r+1 is enqueued before the host
     // waits for round r, so r's tables, keys and flagged count stay untouched
@@ -127,6 +130,7 @@ void serve_free(sw_serve_state* s) {
     dev_free(s->d_counters);
     dev_free(s->d_ovf);
     dev_free(s->d_bnd);
+    dev_free(s->d_segbnd);
     dev_free(s->d_keys[0]);
     dev_free(s->d_keys[1]);
     for (int b = 0; b < 2; ++b) {
@@ -290,7 +294,9 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
         const uint32_t rows = std::max(lanes[2 * d].rows, lanes[2 * d + 1].rows);
         d_nseg.push_back(std::max<uint32_t>(1, (rows + s->pair_seg - 1) / s->pair_seg));
     }
-    auto add_entry = [&](size_t d, uint32_t lv) {
+    std::vector<uint32_t> qp_slot;           // boundary region of each entry
+    auto add_entry = [&](size_t d, uint32_t lv, uint32_t region) {
+        qp_slot.push_back(region);
         uint32_t rs[2];
         for (int h = 0; h < 2; ++h) {
             const uint32_t lr = lanes[2 * d + h].rows;
@@ -312,17 +318,29 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
         QpLaunch L0;
         L0.first = qp_flags.size();
         for (size_t d = 0; d < nd; ++d)
-            if (d_nseg[d] == 1) L0.max_rows = std::max(L0.max_rows, add_entry(d, 0));
+            if (d_nseg[d] == 1) L0.max_rows = std::max(L0.max_rows, add_entry(d, 0, 0));
         L0.count = qp_flags.size() - L0.first;
         if (L0.count) qp_launches.push_back(L0);
+        // taller double stacks in waves of as many as there are boundary
+        // regions, one launch per segment level and wave
+        std::vector<size_t> tall;
         for (size_t d = 0; d < nd; ++d)
-            for (uint32_t lv = 0; d_nseg[d] > 1 && lv < d_nseg[d]; ++lv) {
+            if (d_nseg[d] > 1) tall.push_back(d);
+        const size_t R = (size_t)std::max(s->seg_regions, 1);
+        for (size_t w0 = 0; w0 < tall.size(); w0 += R) {
+            const size_t w1 = std::min(tall.size(), w0 + R);
+            uint32_t levels = 0;
+            for (size_t i = w0; i < w1; ++i) levels = std::max(levels, d_nseg[tall[i]]);
+            for (uint32_t lv = 0; lv < levels; ++lv) {
                 QpLaunch Ls;
                 Ls.first = qp_flags.size();
-                Ls.max_rows = add_entry(d, lv);
-                Ls.count = 1;
+                for (size_t i = w0; i < w1; ++i)
+                    if (lv < d_nseg[tall[i]])
+                        Ls.max_rows = std::max(Ls.max_rows, add_entry(tall[i], lv, (uint32_t)(i - w0)));
+                Ls.count = qp_flags.size() - Ls.first;
                 qp_launches.push_back(Ls);
             }
+        }
     }
     const size_t ne = qp_flags.size();
     // table layout (one upload; the paired block map is read as int2)
@@ -338,7 +356,7 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
     const size_t o_rows = place(4 * finishing.size(), 4);
     const size_t o_qpo0 = place(4 * ne, 4), o_qpr0 = place(4 * ne, 4);
     const size_t o_qpo1 = place(4 * ne, 4), o_qpr1 = place(4 * ne, 4), o_qprb = place(4 * ne, 4);
-    const size_t o_qpfl = place(4 * ne, 4);
+    const size_t o_qpfl = place(4 * ne, 4), o_qpsl = place(4 * ne, 4);
     const size_t o_qpmap = place(4 * qp_rbmap.size(), 8);
     const size_t o_codes = place(codes.size(), 16);
     total = (total + 15) / 16 * 16;
@@ -378,6 +396,7 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
         memcpy(m + o_qpr1, qp_rows[1].data(), 4 * ne);
         memcpy(m + o_qprb, qp_rboff.data(), 4 * ne);
         memcpy(m + o_qpfl, qp_flags.data(), 4 * ne);
+        memcpy(m + o_qpsl, qp_slot.data(), 4 * ne);
         memcpy(m + o_qpmap, qp_rbmap.data(), 4 * qp_rbmap.size());
     }
     if (!codes.empty()) memcpy(m + o_codes, codes.data(), codes.size());
@@ -442,10 +461,13 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
         q.ovf_cap = (int)std::min<size_t>(s->ovf_cap, (size_t)INT32_MAX);
         q.pair_ids = s->d_pair_ids;
         q.seg_flags = base + o_qpfl / 4 + L.first;
-        // a segment's last row for the next segment: the context's per-record
-        // boundary rows (the plain search's; it does not run while a round is
-        // on the stream)
-        q.seg_bnd = ctx->d_bnd;
+        // a segment's last row for the next segment: per-record boundary rows,
+        // one region per double stack of a wave (the serving regions, or the
+        // context's own rows when there is one region: the plain search does
+        // not run while a round is on the stream)
+        q.seg_bnd = s->d_segbnd ? s->d_segbnd : ctx->d_bnd;
+        q.seg_slot = base + o_qpsl / 4 + L.first;
+        q.seg_stride = s->seg_stride;
         void* qargs[] = {&q};
         SW_CUDA(ctx, cudaLaunchKernel(qk->fn, dim3((unsigned)(occq * ctx->num_sms)),
                                       dim3(qk->block), qargs, smem, st));
@@ -931,6 +953,23 @@ extern "C" sw_status sw_serve_start(sw_ctx* ctx, const sw_serve_options* opt) {
         groups = std::max(groups, (size_t)std::max(s->occ_qp_max, 1) * ctx->num_sms *
                                       (qk->block / qk->T));
     if (dev_alloc(&s->d_bnd, groups * s->bnd_group) != cudaSuccess) return fail("boundary rows");
+    if (qk && o.pair_long) {
+        // up to 4 boundary regions (copies of the per-record rows, 8 bytes per
+        // column of every record) so that tall double stacks' segments share
+        // launches, as many as fit in an eighth of the free memory
+        const size_t stride = (size_t)ctx->db_units * 16;
+        size_t fb = 0, tb = 0;
+        if (cudaMemGetInfo(&fb, &tb) != cudaSuccess) cudaGetLastError();
+        const size_t fit = stride ? fb / 8 / (stride * sizeof(uint2)) : 0;
+        const int n = (int)std::min<size_t>(4, fit);
+        if (n > 1 && dev_alloc(&s->d_segbnd, (size_t)n * stride) == cudaSuccess) {
+            s->seg_regions = n;
+            s->seg_stride = stride;
+        } else {
+            cudaGetLastError();
+            s->d_segbnd = nullptr;
+        }
+    }
     for (int b = 0; b < 2; ++b) {
         if (cudaMallocHost((void**)&s->h_keys[b],
                            (size_t)s->n_slots * ctx->params.top_k * sizeof(unsigned long long)) !=
