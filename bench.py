@@ -78,6 +78,12 @@ def parse(argv=None):
                     help="requests per offered load in the serving leg (0 = skip it)")
     ap.add_argument("--serve-levels", type=str, default="0.25,0.5,0.75,1.0",
                     help="offered loads of the serving leg, as fractions of the saturating rate")
+    ap.add_argument("--serve-chunks", type=int, default=None,
+                    help="serving: DB chunks of the ring (default: the library's)")
+    ap.add_argument("--serve-slots", type=int, default=None,
+                    help="serving: requests in flight (default: the library's)")
+    ap.add_argument("--serve-pair-long", type=int, choices=[0, 1], default=None,
+                    help="serving: pair long requests too (default: the library's)")
     ap.add_argument("--no-stress", action="store_true",
                     help="skip the overflow / long-record stress measurement")
     ap.add_argument("--kernel-only", action="store_true",
@@ -309,7 +315,7 @@ def run_reference(args, rank, world):
 
 
 # ---------------------------------------------------------------------------
-def serve_leg(ctx, db, n_req: int, seed: int = 5, loads=(0.25, 0.5, 0.75, 1.0)):
+def serve_leg(ctx, db, n_req: int, seed: int = 5, loads=(0.25, 0.5, 0.75, 1.0), opts=None):
     """Serving: requests of lengths log-uniform 30..8,000 (seeded) against the
     resident DB through sw_serve_*.  First the saturating rate (3x the slot
     count submitted at once), then Poisson arrivals at 25/50/75/100% of it,
@@ -329,7 +335,7 @@ def serve_leg(ctx, db, n_req: int, seed: int = 5, loads=(0.25, 0.5, 0.75, 1.0)):
                 got[r["id"]] = r
         return got
 
-    ctx.serve_start()
+    ctx.serve_start(**(opts or {}))
     try:
         slots = int(ctx.serve_stats().slots)
         # saturating rate: a full queue, throughput from first submit to last completion
@@ -600,7 +606,11 @@ def run_ours(args, rank, world, local_rank):
     if args.workload == "full" and args.serve_requests > 0:
         ctx.set_stream(None)
         served = serve_leg(ctx, db, args.serve_requests,
-                           loads=tuple(float(x) for x in args.serve_levels.split(",")))
+                           loads=tuple(float(x) for x in args.serve_levels.split(",") if x),
+                           opts={k: v for k, v in (("chunks", args.serve_chunks),
+                                                   ("max_active", args.serve_slots),
+                                                   ("pair_long", args.serve_pair_long))
+                                 if v is not None})
 
     # ---- overflow / long-record stress (its own DB and context) ----
     stress = None
