@@ -624,22 +624,15 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
             std::vector<uint32_t> q;
             uint32_t rows = 0;
         };
+        std::vector<uint32_t> need_rows;
+        for (uint32_t i = ip; i < nz; ++i) need_rows.push_back((qlen[order[i]] + qR - 1) / qR * qR);
         std::vector<Lane> lanes;
-        for (uint32_t i = ip; i < nz; ++i) {
-            const uint32_t q = order[i];
-            const uint32_t need = (qlen[q] + qR - 1) / qR * qR;
-            bool placed = false;
-            if (need <= seg)
-                for (Lane& ln : lanes)
-                    if (ln.rows + need <= seg) {
-                        ln.q.push_back(q);
-                        ln.rows += need;
-                        placed = true;
-                        break;
-                    }
-            if (!placed) lanes.push_back(Lane{{q}, need});
+        for (const PairLane& pl : plan_pair_lanes(need_rows, seg, pass_rows)) {
+            Lane ln;
+            for (const uint32_t it : pl.items) ln.q.push_back(order[ip + it]);
+            ln.rows = pl.rows;
+            lanes.push_back(ln);
         }
-        if (lanes.size() % 2) lanes.push_back(Lane{});      // an empty high lane
         struct Double {
             uint32_t off[2], rows[2], nseg;
             std::vector<int32_t> blocks[2];

@@ -21,6 +21,8 @@
 // code (a pair of int16 scores), 4 rows per 16-byte word, so a double stack
 // holds at most ~2,200 rows in shared memory.
 #pragma once
+#include <algorithm>
+#include <vector>
 #include "sw_device.cuh"
 #include "sw_wavefront.cuh"
 
@@ -63,6 +65,66 @@ struct QpArgs {
     const uint32_t* seg_slot;
     size_t seg_stride;
 };
+
+// Host planning of paired lanes (batched search and serving).  Items (queries)
+// come longest first with their rows padded to whole R-row blocks (`need`).
+// An item taller than `seg` gets a lane of its own; those lanes are paired
+// first (with an empty partner when their number is odd), and since a double
+// stack computes whole passes of `pass_rows` rows, each of its lanes is then
+// filled up to that height with the short items (first fit, longest first),
+// rows that would otherwise be padding.  The remaining short items fill lanes
+// of at most `seg` rows.  Consecutive lanes of the result form the double
+// stacks (an even number of lanes).
+struct PairLane {
+    std::vector<uint32_t> items;
+    uint32_t rows = 0;
+};
+
+inline std::vector<PairLane> plan_pair_lanes(const std::vector<uint32_t>& need, uint32_t seg,
+                                             uint32_t pass_rows) {
+    std::vector<PairLane> tall, shortl;
+    std::vector<uint32_t> rest;
+    for (uint32_t i = 0; i < (uint32_t)need.size(); ++i) {
+        if (need[i] > seg) {
+            PairLane ln;
+            ln.items.push_back(i);
+            ln.rows = need[i];
+            tall.push_back(ln);
+        } else {
+            rest.push_back(i);
+        }
+    }
+    if (tall.size() % 2) tall.push_back(PairLane{});
+    std::vector<uint32_t> cap(tall.size());
+    for (size_t d = 0; d + 1 < tall.size(); d += 2) {
+        const uint32_t h = std::max(tall[d].rows, tall[d + 1].rows);
+        cap[d] = cap[d + 1] = (h + pass_rows - 1) / pass_rows * pass_rows;
+    }
+    for (const uint32_t i : rest) {
+        bool placed = false;
+        for (size_t l = 0; l < tall.size() && !placed; ++l)
+            if (tall[l].rows + need[i] <= cap[l]) {
+                tall[l].items.push_back(i);
+                tall[l].rows += need[i];
+                placed = true;
+            }
+        for (size_t l = 0; l < shortl.size() && !placed; ++l)
+            if (shortl[l].rows + need[i] <= seg) {
+                shortl[l].items.push_back(i);
+                shortl[l].rows += need[i];
+                placed = true;
+            }
+        if (!placed) {
+            PairLane ln;
+            ln.items.push_back(i);
+            ln.rows = need[i];
+            shortl.push_back(ln);
+        }
+    }
+    if (shortl.size() % 2) shortl.push_back(PairLane{});
+    tall.insert(tall.end(), shortl.begin(), shortl.end());
+    return tall;
+}
 
 // Shared-memory bytes of a double stack's profile (rows = the taller lane).
 template <int T, int R>

@@ -238,27 +238,27 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
         for (uint32_t j = 0; j < P * (uint32_t)T; ++j)
             rbmap.push_back(j < block_q.size() ? block_q[j] : -1);
     }
-    // paired lanes: first fit (longest first) into lanes of at most pair_seg
-    // rows, each request padded to whole R-row blocks; consecutive lanes form
-    // a double stack (low lane, high lane)
+    // paired lanes (plan_pair_lanes, sw_qpair.cuh): a request longer than
+    // pair_seg rows gets a lane of its own, the others fill the rows the
+    // tall double stacks' last passes would leave as padding, then lanes of
+    // at most pair_seg rows; each request padded to whole R-row blocks;
+    // consecutive lanes form a double stack (low lane, high lane)
     struct Lane {
         std::vector<int> slots;
         uint32_t rows = 0;
     };
     std::vector<Lane> lanes;
-    for (int sl : paired) {
-        const uint32_t need = ((uint32_t)s->slots[sl].req.query.size() + qR - 1) / qR * qR;
-        bool placed = false;
-        for (Lane& ln : lanes)
-            if (ln.rows + need <= s->pair_seg) {
-                ln.slots.push_back(sl);
-                ln.rows += need;
-                placed = true;
-                break;
-            }
-        if (!placed) lanes.push_back(Lane{{sl}, need});
+    {
+        std::vector<uint32_t> need_rows;
+        for (int sl : paired)
+            need_rows.push_back(((uint32_t)s->slots[sl].req.query.size() + qR - 1) / qR * qR);
+        for (const PairLane& pl : plan_pair_lanes(need_rows, s->pair_seg, qT * qR)) {
+            Lane ln;
+            for (const uint32_t it : pl.items) ln.slots.push_back(paired[it]);
+            ln.rows = pl.rows;
+            lanes.push_back(ln);
+        }
     }
-    if (lanes.size() % 2) lanes.push_back(Lane{});
     const size_t nd = lanes.size() / 2;
     // entries of the paired launches: one per (double stack, segment); every
     // single-segment double stack in the first launch, then each taller one's
