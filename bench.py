@@ -84,6 +84,8 @@ def parse(argv=None):
                     help="serving: requests in flight (default: the library's)")
     ap.add_argument("--serve-pair-long", type=int, choices=[0, 1], default=None,
                     help="serving: pair long requests too (default: the library's)")
+    ap.add_argument("--serve-regions", type=int, default=None,
+                    help="serving: boundary regions of tall paired lanes (default: the library's)")
     ap.add_argument("--no-stress", action="store_true",
                     help="skip the overflow / long-record stress measurement")
     ap.add_argument("--kernel-only", action="store_true",
@@ -340,11 +342,13 @@ def serve_leg(ctx, db, n_req: int, seed: int = 5, loads=(0.25, 0.5, 0.75, 1.0), 
         slots = int(ctx.serve_stats().slots)
         # saturating rate: a full queue, throughput from first submit to last completion
         sat_q = requests(3 * slots)
+        st_a = ctx.serve_stats()
         t0 = capi.serve_clock_ms()
         for i, q in enumerate(sat_q):
             ctx.serve_submit(i, q)
         got = collect(len(sat_q), 600)
         t1 = max(r["done_ms"] for r in got.values())
+        st_b = ctx.serve_stats()
         sat_cells = sum(len(q) for q in sat_q) * db.total
         sat_rate = len(sat_q) / ((t1 - t0) * 1e-3)
         levels = []
@@ -378,6 +382,7 @@ def serve_leg(ctx, db, n_req: int, seed: int = 5, loads=(0.25, 0.5, 0.75, 1.0), 
                 "latency_ms_p999": round(float(np.percentile(lat, 99.9)), 1),
                 "queue_wait_ms_p50": round(float(np.percentile(wait, 50)), 1),
                 "gcups": round(cells / ((last - first) * 1e-3) / 1e9, 1),
+                "device_ms": round(st1.device_ms - st0.device_ms, 1),
                 "rounds": int(st1.rounds - st0.rounds),
                 "launches": int(st1.launches - st0.launches),
             })
@@ -396,7 +401,13 @@ def serve_leg(ctx, db, n_req: int, seed: int = 5, loads=(0.25, 0.5, 0.75, 1.0), 
                         3 * slots, "/".join(f"{100 * f:g}" for f in loads), n_req),
         "slots": slots, "chunks": int(st.chunks),
         "saturated": {"requests": len(sat_q), "rate_per_s": round(sat_rate, 3),
-                      "gcups": round(sat_cells / ((t1 - t0) * 1e-3) / 1e9, 1)},
+                      "gcups": round(sat_cells / ((t1 - t0) * 1e-3) / 1e9, 1),
+                      "wall_ms": round(t1 - t0, 1),
+                      "device_ms": round(st_b.device_ms - st_a.device_ms, 1),
+                      "device_gcups": round(sat_cells / max(st_b.device_ms - st_a.device_ms,
+                                                            1e-9) * 1e-6, 1),
+                      "rounds": int(st_b.rounds - st_a.rounds),
+                      "launches": int(st_b.launches - st_a.launches)},
         "levels": levels,
         "top10_equal_plain": {"checked": len(check_ids), "all_equal": bool(exact)},
         "rescored": int(st.rescored),
@@ -609,7 +620,8 @@ def run_ours(args, rank, world, local_rank):
                            loads=tuple(float(x) for x in args.serve_levels.split(",") if x),
                            opts={k: v for k, v in (("chunks", args.serve_chunks),
                                                    ("max_active", args.serve_slots),
-                                                   ("pair_long", args.serve_pair_long))
+                                                   ("pair_long", args.serve_pair_long),
+                                                   ("pair_regions", args.serve_regions))
                                  if v is not None})
 
     # ---- overflow / long-record stress (its own DB and context) ----

@@ -319,6 +319,10 @@ typedef struct sw_batch_options {
     int32_t pair_rows_per_thread;
     int32_t pair_long;      /* != 0: longer queries are paired too (a lane each, scored in
                                segments of pair_rows rows by consecutive launches) */
+    int32_t pair_regions;   /* boundary regions for those segments: up to this many tall
+                               double stacks share each segment launch (a region holds
+                               8 bytes per DB column); 0 = automatic: up to 16, as many
+                               as fit in a quarter of the free memory */
 } sw_batch_options;
 
 /* NULL restores the defaults (no cut-over, long shape 32x16, graphs on,
@@ -401,11 +405,16 @@ typedef struct sw_serve_options {
     int32_t pair_rows_per_thread;
     int32_t pair_long;        /* != 0: longer requests are paired too (a lane each, scored
                                  in pair_rows-row segments by consecutive launches) */
+    int32_t pair_regions;     /* boundary regions for those segments: up to this many
+                                 tall double stacks share each segment launch (a region
+                                 holds 8 bytes per DB column); 0 = automatic: up to 16,
+                                 as many as fit in an eighth of the free memory */
 } sw_serve_options;
 
 /* Defaults: 128 slots, 4 chunks, unbounded queue, half the free memory,
  * shape 16x64, stacks of 4096 rows, every request paired two per register
- * with shape 16x64, in lanes of up to 2048 rows (as sw_search_batch does). */
+ * with shape 16x64, in lanes of up to 2048 rows (as sw_search_batch does),
+ * automatic boundary regions. */
 void sw_serve_options_default(sw_serve_options *opt);
 
 typedef struct sw_serve_result {
@@ -424,6 +433,9 @@ typedef struct sw_serve_stats {
     double busy_ms;           /* wall time inside device rounds */
     uint32_t slots, chunks;   /* as sized by sw_serve_start */
     uint32_t active, pending; /* now */
+    double device_ms;         /* device time of the rounds (CUDA events from each round's
+                                 table upload to its result download); busy_ms minus this
+                                 is time the device waited for the host */
 } sw_serve_stats;
 
 /* Starts the scheduler thread (opt NULL = defaults).  The slot count is

@@ -71,7 +71,7 @@ class sw_batch_options(ctypes.Structure):
                 ("group_width", ctypes.c_int32), ("rows_per_thread", ctypes.c_int32),
                 ("stack_rows", ctypes.c_int32), ("pair_rows", ctypes.c_int32),
                 ("pair_group_width", ctypes.c_int32), ("pair_rows_per_thread", ctypes.c_int32),
-                ("pair_long", ctypes.c_int32)]
+                ("pair_long", ctypes.c_int32), ("pair_regions", ctypes.c_int32)]
 
 
 class sw_image_info(ctypes.Structure):
@@ -95,7 +95,7 @@ class sw_serve_options(ctypes.Structure):
                 ("group_width", ctypes.c_int32), ("rows_per_thread", ctypes.c_int32),
                 ("stack_rows", ctypes.c_int32), ("pair_rows", ctypes.c_int32),
                 ("pair_group_width", ctypes.c_int32), ("pair_rows_per_thread", ctypes.c_int32),
-                ("pair_long", ctypes.c_int32)]
+                ("pair_long", ctypes.c_int32), ("pair_regions", ctypes.c_int32)]
 
 
 class sw_serve_result(ctypes.Structure):
@@ -111,7 +111,7 @@ class sw_serve_stats(ctypes.Structure):
                 ("rescored", ctypes.c_uint64), ("cells", ctypes.c_uint64),
                 ("busy_ms", ctypes.c_double), ("slots", ctypes.c_uint32),
                 ("chunks", ctypes.c_uint32), ("active", ctypes.c_uint32),
-                ("pending", ctypes.c_uint32)]
+                ("pending", ctypes.c_uint32), ("device_ms", ctypes.c_double)]
 
 
 class sw_tuning_entry(ctypes.Structure):
@@ -429,10 +429,10 @@ class Context:
 
     def set_batch_options(self, cutover=0, long_shape=(32, 16), use_graph=True,
                           stack_shape=(16, 64), stack_rows=4096, pair_rows=2048,
-                          pair_shape=(16, 64), pair_long=True):
+                          pair_shape=(16, 64), pair_long=True, pair_regions=0):
         o = sw_batch_options(cutover, long_shape[0], long_shape[1], 1 if use_graph else 0,
                              stack_shape[0], stack_shape[1], stack_rows, pair_rows,
-                             pair_shape[0], pair_shape[1], 1 if pair_long else 0)
+                             pair_shape[0], pair_shape[1], 1 if pair_long else 0, pair_regions)
         self._check(self.L.sw_set_batch_options(self.h, ctypes.byref(o)), "sw_set_batch_options")
 
     def search_batch(self, queries, want_scores: bool = False):
@@ -516,7 +516,7 @@ class Context:
     # ---- serving ----------------------------------------------------------
     def serve_start(self, max_active=None, chunks=None, max_pending=None, memory_budget=None,
                     shape=None, stack_rows=None, pair_rows=None, pair_shape=None,
-                    pair_long=None):
+                    pair_long=None, pair_regions=None):
         o = sw_serve_options()
         self.L.sw_serve_options_default(ctypes.byref(o))
         if max_active is not None:
@@ -537,6 +537,8 @@ class Context:
             o.pair_group_width, o.pair_rows_per_thread = pair_shape
         if pair_long is not None:
             o.pair_long = 1 if pair_long else 0
+        if pair_regions is not None:
+            o.pair_regions = pair_regions
         self._check(self.L.sw_serve_start(self.h, ctypes.byref(o)), "sw_serve_start")
 
     def serve_submit(self, request_id: int, query: np.ndarray) -> int:

@@ -47,6 +47,8 @@ struct BatchLaunch {
     int counter_base;          // first counter of this launch
     bool long_part;            // runs on the side stream
     size_t bnd_group;
+    int long_units = 0;        // paired: units of the long phase (QpArgs::long_units) ...
+    int long_ordinal = 0;      // ... and its counter, after the entries' counters
 };
 
 // Host image of a batch's stacks (uploaded as one block, see enqueue_batch).
@@ -76,7 +78,7 @@ struct BatchGraph {
 };
 
 struct sw_batch_state {
-    sw_batch_options opt{0, 32, 16, 1, 16, 64, 4096, 2048, 16, 64, 1};
+    sw_batch_options opt{0, 32, 16, 1, 16, 64, 4096, 2048, 16, 64, 1, 0};
     // device
     uint8_t* d_queries = nullptr;
     size_t queries_cap = 0;
@@ -152,7 +154,7 @@ double wall_ms() {
 }
 
 // Boundary regions for `want` tall double stacks whose segments share
-// launches: at most 4, as many as fit in a quarter of the free device memory
+// launches: at most `want`, as many as fit in a quarter of the free device memory
 // (each is a copy of the context's per-record boundary rows, 8 bytes per
 // column of every record); 1 means the context's own rows.  Grows (never
 // shrinks) the batch state's region buffer; called before any capture.
@@ -169,7 +171,7 @@ int seg_regions_for(sw_ctx* ctx, sw_batch_state* b, int want) {
         b->seg_regions = 1;
         b->seg_stride = 0;
     }
-    want = std::max(1, std::min(want, 4));
+    want = std::max(1, want);
     if (want <= 1 || stride == 0) return 1;
     if (b->seg_regions >= want && b->seg_stride == stride) return want;
     size_t free_b = 0, total_b = 0;
@@ -250,8 +252,10 @@ sw_status enqueue_batch(sw_ctx* ctx, sw_batch_state* b, uint32_t nq, size_t qbyt
     SW_CUDA(ctx, cudaMemcpyAsync(b->d_meta, b->h_stage + meta_at, ml.total,
                                  cudaMemcpyHostToDevice, st));
     const int nst = ml.nst;
-    SW_CUDA(ctx, cudaMemsetAsync(b->d_counters, 0, (2 * (size_t)nst + 1 + ml.nqp) * sizeof(int),
-                                 st));
+    int n_qp_launches = 0;
+    for (const BatchLaunch& L : launches) n_qp_launches += L.qk ? 1 : 0;
+    SW_CUDA(ctx, cudaMemsetAsync(b->d_counters, 0,
+                                 (2 * (size_t)nst + 1 + ml.nqp + n_qp_launches) * sizeof(int), st));
     SW_CUDA(ctx, cudaMemsetAsync(b->d_scores, 0, (size_t)nq * n_rec * sizeof(int), st));
     const uint32_t* d_qoff = reinterpret_cast<const uint32_t*>(b->d_meta + ml.qoff);
     const uint32_t* d_qlen = reinterpret_cast<const uint32_t*>(b->d_meta + ml.qlen);
@@ -297,6 +301,8 @@ sw_status enqueue_batch(sw_ctx* ctx, sw_batch_state* b, uint32_t nq, size_t qbyt
             q.seg_bnd = b->d_segbnd ? b->d_segbnd : ctx->d_bnd;
             q.seg_slot = reinterpret_cast<const uint32_t*>(b->d_meta + ml.qp_slot) + L.sbegin;
             q.seg_stride = b->seg_stride;
+            q.long_units = L.long_units;
+            q.long_counter = b->d_counters + 2 * nst + 1 + ml.nqp + L.long_ordinal;
             void* args[] = {&q};
             SW_CUDA(ctx, cudaLaunchKernel(L.qk->fn, dim3((unsigned)L.grid), dim3(L.threads), args,
                                           L.smem, st));
@@ -419,12 +425,12 @@ extern "C" sw_status sw_set_batch_options(sw_ctx* ctx, const sw_batch_options* o
     if (opt) {
         if (opt->cutover < 0 || !find_kernel(opt->long_group_width, opt->long_rows_per_thread) ||
             !find_kernel(opt->group_width, opt->rows_per_thread) || opt->stack_rows < 0 ||
-            opt->pair_rows < 0 ||
+            opt->pair_rows < 0 || opt->pair_regions < 0 ||
             (opt->pair_rows > 0 && !find_qp(opt->pair_group_width, opt->pair_rows_per_thread)))
             SW_SET(ctx, SW_ERR_INVALID, "bad batch options");
         ctx->batch->opt = *opt;
     } else {
-        ctx->batch->opt = sw_batch_options{0, 32, 16, 1, 16, 64, 4096, 2048, 16, 64, 1};
+        ctx->batch->opt = sw_batch_options{0, 32, 16, 1, 16, 64, 4096, 2048, 16, 64, 1, 0};
     }
     for (auto& kv : ctx->batch->graphs) {
         if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
@@ -540,6 +546,7 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
     StackPlan sp;
     std::vector<BatchLaunch> launches;
     size_t bnd_long = 0, bnd_bulk = 0;
+    int n_qp_launches = 0;
     int nst_total = 0;
     for (const Bucket& bk : buckets) nst_total += (int)bk.stacks.size();
     int sidx = 0;
@@ -665,7 +672,8 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
         std::vector<size_t> tall;
         for (size_t d = 0; d < dbl.size(); ++d)
             if (dbl[d].nseg > 1) tall.push_back(d);
-        const int regions = seg_regions_for(ctx, b, (int)tall.size());
+        const int regions = seg_regions_for(
+            ctx, b, std::min((int)tall.size(), b->opt.pair_regions > 0 ? b->opt.pair_regions : 16));
         // (double stack, segment, region)
         std::vector<std::vector<std::array<uint32_t, 3>>> groups(1);
         for (size_t d = 0; d < dbl.size(); ++d)
@@ -729,12 +737,18 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
             L.counter_base = 2 * nst_total + 1 + first;
             L.long_part = false;
             L.bnd_group = 2 * (size_t)ctx->max_cols;
+            L.long_units = qp_long_units(
+                [&](int p) { return (uint64_t)ctx->pair_ncols[(size_t)p]; },
+                (int)ctx->n_pairs, ctx->pair_cols_total,
+                (long long)L.grid * (L.threads / qk->T));
+            L.long_ordinal = n_qp_launches++;
             bnd_bulk = std::max(bnd_bulk, (size_t)L.grid * (L.threads / qk->T) * L.bnd_group);
             launches.push_back(L);
         }
     }
     // counters: bulk of stack i at [i], long at [nst_total + i], overflow count
-    // at [2 nst_total], paired double stack j at [2 nst_total + 1 + j]
+    // at [2 nst_total], paired double stack j at [2 nst_total + 1 + j], the
+    // long phase of paired launch l at [2 nst_total + 1 + nqp + l]
     const MetaLayout ml = meta_layout(nq, sp);
 
     // ---- buffers (before any capture) ----
@@ -747,7 +761,7 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
         }
         b->graphs.clear();
     };
-    const size_t counters_need = 2 * (size_t)nst_total + 1 + ml.nqp;
+    const size_t counters_need = 2 * (size_t)nst_total + 1 + ml.nqp + n_qp_launches;
     if (std::max<uint64_t>(qbytes, 1) > b->queries_cap || ml.total > b->meta_cap ||
         counters_need > b->counters_cap)
         drop_graphs();
@@ -846,6 +860,7 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
     sig.push_back((uint64_t)b->opt.pair_rows << 32 |
                   (uint64_t)(b->opt.pair_group_width * 256 + b->opt.pair_rows_per_thread) << 1 |
                   (uint64_t)(b->opt.pair_long != 0));
+    sig.push_back((uint64_t)b->opt.pair_regions);
     for (uint32_t i = 0; i < nq; ++i) sig.push_back(qlen[i]);
     uint32_t n_launch = 0;
     SW_CUDA(ctx, cudaEventRecord(ctx->ev[0], ctx->stream));

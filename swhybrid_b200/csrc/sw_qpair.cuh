@@ -64,6 +64,12 @@ struct QpArgs {
     // boundary region seg_bnd + seg_slot[i] * seg_stride (null: region 0)
     const uint32_t* seg_slot;
     size_t seg_stride;
+    // units [0, long_units) are the launch's long records (longest first):
+    // they are scored before the rest, in items of one unit per group of a
+    // block, all from one double stack (long_counter: items claimed, zero
+    // before), so no block holds its groups at a stack's end for one long unit
+    int long_units;
+    int* long_counter;
 };
 
 // Host planning of paired lanes (batched search and serving).  Items (queries)
@@ -124,6 +130,26 @@ inline std::vector<PairLane> plan_pair_lanes(const std::vector<uint32_t>& need, 
     if (shortl.size() % 2) shortl.push_back(PairLane{});
     tall.insert(tall.end(), shortl.begin(), shortl.end());
     return tall;
+}
+
+// QpArgs::long_units of a launch over `count` pairs, longest first, whose
+// column counts are ncols(p) and sum to cols_total, run by `groups` groups:
+// both units of every leading pair longer than half of one group's share of
+// a double stack (2 cols_total / groups).  A shorter unit, claimed at a
+// stack's start, ends before the stack's other units run out.
+template <class NCols>
+inline int qp_long_units(NCols ncols, int count, uint64_t cols_total, long long groups) {
+    if (count <= 0 || groups <= 0) return 0;
+    const uint64_t thr = cols_total / (uint64_t)groups;
+    int lo = 0, hi = count;            // the first pair with ncols <= thr
+    while (lo < hi) {
+        const int mid = lo + (hi - lo) / 2;
+        if ((uint64_t)ncols(mid) > thr)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return 2 * lo;
 }
 
 // Shared-memory bytes of a double stack's profile (rows = the taller lane).
@@ -231,9 +257,14 @@ __device__ __forceinline__ void column_step_qp(uint32_t (&H)[R], uint32_t (&E)[R
 // seg), and the last pass writes its last row there for the next segment
 // (bit 1): a column is read (pass 0, thread 0) 2T + 1 steps before the last
 // pass's thread T-1 writes it, so one buffer serves both.
+//
+// Units come from `counter` (unit_first + claims, up to units_end) or, with a
+// null counter, the group scores the one unit `single` (none when single >=
+// units_end).
 template <int T, int R>
 __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, int P, int* counter,
-                                           const int2* rb_map, uint32_t seg, size_t seg_base) {
+                                           const int2* rb_map, uint32_t seg, size_t seg_base,
+                                           int unit_first, int units_end, int single) {
     static_assert(R % 8 == 0, "R");
     constexpr int NJ = R / 4;
     constexpr int HALF = R / 2;
@@ -251,8 +282,15 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
     K.neg_e2 = a.neg_e;
     const uint32_t Z = a.bias2;
     const int bias = (int)(a.bias2 & 0xffffu);
-    const int units = 2 * a.pair_count;
+    const int units = units_end;
     const int dep_steps = 2 * T + 2;
+    // thread 0 claims the group's units
+    auto claim = [&]() -> int {
+        if (counter) return unit_first + atomicAdd(counter, 1);
+        const int v = single;
+        single = units;
+        return v;
+    };
     uint2* const pbnd = a.bnd + (size_t)((blockIdx.x * blockDim.x + threadIdx.x) / T) * a.bnd_group;
 
     uint32_t H[R], E[R];
@@ -312,7 +350,7 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
 
     {
         int v = 0;
-        if (t == 0) v = atomicAdd(counter, 1);
+        if (t == 0) v = claim();
         v = __shfl_sync(gmask, v, 0, T);
         unit = v;
         if (v < units) {
@@ -320,7 +358,7 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
             off16 = pr.off16;
             ncols = (int)pr.ncols;
             half = v & 1;
-            if (t == 0) next = atomicAdd(counter, 1);
+            if (t == 0) next = claim();
         } else {
             fin = true;
         }
@@ -437,7 +475,7 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
                         unit = next;
                         off16 = ninfo.off16;
                         ncols = (int)ninfo.ncols;
-                        if (unit < units) next = atomicAdd(counter, 1);
+                        if (unit < units) next = claim();
                     } else {
                         unit = up_unit;
                         off16 = up_off;
@@ -512,20 +550,54 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
 #undef SWQ_SET_SEG
 }
 
-// The paired-query batched kernel: blocks walk the double stacks in order.
+// The paired-query batched kernel.  First the long units: a block claims
+// items of G = BLOCK / T consecutive long units of one double stack (similar
+// lengths, the pair table being longest first), one per group; then the
+// blocks walk the double stacks in order, claiming the other units.
 template <int T, int R, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1) sw_qpbatch(const QpArgs a) {
     extern __shared__ uint4 prof4[];
-    for (int i = 0; i < a.nstacks; ++i) {
+    __shared__ int s_item;
+    constexpr int G = BLOCK / T;
+    const int units = 2 * a.pair_count;
+    const int n_long = min(a.long_units, units);
+    int cur = -1;               // the double stack whose profile is in shared memory
+    auto stage = [&](int i) {   // caller: every group is done with the previous profile
         const int rows = (int)max(a.rows_lo[i], a.rows_hi[i]);
         const int P = (rows + T * R - 1) / (T * R);
-        __syncthreads();        // every group is done with the previous profile
-        build_profile_qp<T, R>(prof4, a.codes + a.off_lo[i], (int)a.rows_lo[i],
-                               a.codes + a.off_hi[i], (int)a.rows_hi[i], a.mat, P);
+        if (i != cur) {
+            build_profile_qp<T, R>(prof4, a.codes + a.off_lo[i], (int)a.rows_lo[i],
+                                   a.codes + a.off_hi[i], (int)a.rows_hi[i], a.mat, P);
+            cur = i;
+        }
         __syncthreads();
+        return P;
+    };
+    if (n_long > 0) {
+        const int per = (n_long + G - 1) / G;
+        const int items = per * a.nstacks;
+        while (true) {
+            __syncthreads();    // the previous item is done and s_item was read
+            if (threadIdx.x == 0) s_item = atomicAdd(a.long_counter, 1);
+            __syncthreads();
+            const int it = s_item;
+            if (it >= items) break;
+            const int i = it / per;
+            const int u = (it - i * per) * G + (int)threadIdx.x / T;
+            const int P = stage(i);
+            run_qpairs<T, R>(a, prof4, P, nullptr, a.rb_map + a.rb_off[i],
+                             a.seg_flags ? a.seg_flags[i] : 0u,
+                             a.seg_slot ? (size_t)a.seg_slot[i] * a.seg_stride : (size_t)0, 0,
+                             n_long, u);
+        }
+    }
+    for (int i = 0; i < a.nstacks; ++i) {
+        __syncthreads();        // every group is done with the previous profile
+        const int P = stage(i);
         run_qpairs<T, R>(a, prof4, P, a.counters + i, a.rb_map + a.rb_off[i],
                          a.seg_flags ? a.seg_flags[i] : 0u,
-                         a.seg_slot ? (size_t)a.seg_slot[i] * a.seg_stride : (size_t)0);
+                         a.seg_slot ? (size_t)a.seg_slot[i] * a.seg_stride : (size_t)0, n_long,
+                         units, 0);
     }
 }
 

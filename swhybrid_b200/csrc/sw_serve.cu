@@ -88,6 +88,8 @@ struct sw_serve_state {
     int occ_max = 0;                      // most blocks per SM any stack height gives
     int occ_qp_max = 0;                   // ... and any paired lane height
     std::vector<int> chunk_begin;         // n_chunks + 1 entries into d_pairs
+    std::vector<uint32_t> ring_ncols;     // column count of each entry of d_pairs
+    std::vector<uint64_t> chunk_cols;     // sum of ring_ncols per chunk
     Pair2* d_pairs = nullptr;             // pair table, chunk after chunk
     uint32_t* d_pair_ids = nullptr;       // global pair index of each entry
     int* d_scores = nullptr;              // [slot][sorted position]
@@ -110,6 +112,7 @@ struct sw_serve_state {
     unsigned long long* h_keys[2] = {nullptr, nullptr}; // pinned: n_slots * top_k
     int* h_flagged[2] = {nullptr, nullptr};            // pinned: the round's overflow count
     cudaEvent_t done_ev[2] = {nullptr, nullptr};       // the round's last operation
+    cudaEvent_t start_ev[2] = {nullptr, nullptr};      // the round's first operation
     int cursor = 0;                       // next chunk of the ring
     std::vector<Slot> slots;
     std::deque<Request> pending, done;
@@ -138,10 +141,12 @@ void serve_free(sw_serve_state* s) {
         if (s->h_keys[b]) cudaFreeHost(s->h_keys[b]);
         if (s->h_flagged[b]) cudaFreeHost(s->h_flagged[b]);
         if (s->done_ev[b]) cudaEventDestroy(s->done_ev[b]);
+        if (s->start_ev[b]) cudaEventDestroy(s->start_ev[b]);
         s->h_stage[b] = nullptr;
         s->h_keys[b] = nullptr;
         s->h_flagged[b] = nullptr;
         s->done_ev[b] = nullptr;
+        s->start_ev[b] = nullptr;
         s->stage_cap[b] = 0;
     }
 }
@@ -400,6 +405,7 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
         memcpy(m + o_qpmap, qp_rbmap.data(), 4 * qp_rbmap.size());
     }
     if (!codes.empty()) memcpy(m + o_codes, codes.data(), codes.size());
+    SW_CUDA(ctx, cudaEventRecord(s->start_ev[buf], st));
     SW_CUDA(ctx, cudaMemcpyAsync(s->d_meta, m, total, cudaMemcpyHostToDevice, st));
     // score rows of requests admitted at this boundary start at zero (atomicMax)
     for (int sl : active)
@@ -407,17 +413,19 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
             SW_CUDA(ctx, cudaMemsetAsync(s->d_scores + (size_t)sl * n_rec, 0,
                                          (size_t)n_rec * sizeof(int), st));
     // counters: stack i at [i], the overflow count at [ns], paired entry j at
-    // [ns + 1 + j]
-    if (ns + 1 + ne > s->counters_cap)
+    // [ns + 1 + j], the long phase of paired launch l at [ns + 1 + ne + l]
+    const size_t n_counters = ns + 1 + ne + qp_launches.size();
+    if (n_counters > s->counters_cap)
         SW_SET(ctx, SW_ERR_UNSUPPORTED, "%zu paired launch entries exceed the counters (%zu)", ne,
                s->counters_cap);
-    SW_CUDA(ctx, cudaMemsetAsync(s->d_counters, 0, (ns + 1 + ne) * sizeof(int), st));
+    SW_CUDA(ctx, cudaMemsetAsync(s->d_counters, 0, n_counters * sizeof(int), st));
     const int occ = ns ? std::min(shape_occupancy(ctx, *s->k, (int)max_rows), s->occ_max) : 1;
     if (occ <= 0)
         SW_SET(ctx, SW_ERR_UNSUPPORTED, "a stack of %u rows does not fit shape %dx%d", max_rows,
                T, R);
     int* d_ovf_count = s->d_counters + ns;
     const int pair_count = s->chunk_begin[chunk + 1] - s->chunk_begin[chunk];
+    size_t qp_ordinal = 0;
     for (const QpLaunch& L : pair_count > 0 ? qp_launches : std::vector<QpLaunch>()) {
         const size_t smem = qk->smem((int)std::max<uint32_t>(L.max_rows, 1));
         int occq = 0;
@@ -468,6 +476,11 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
         q.seg_bnd = s->d_segbnd ? s->d_segbnd : ctx->d_bnd;
         q.seg_slot = base + o_qpsl / 4 + L.first;
         q.seg_stride = s->seg_stride;
+        const int cb = s->chunk_begin[chunk];
+        q.long_units = qp_long_units([&](int p) { return (uint64_t)s->ring_ncols[(size_t)(cb + p)]; },
+                                     pair_count, s->chunk_cols[(size_t)chunk],
+                                     (long long)occq * ctx->num_sms * (qk->block / qk->T));
+        q.long_counter = s->d_counters + ns + 1 + ne + qp_ordinal++;
         void* qargs[] = {&q};
         SW_CUDA(ctx, cudaLaunchKernel(qk->fn, dim3((unsigned)(occq * ctx->num_sms)),
                                       dim3(qk->block), qargs, smem, st));
@@ -578,10 +591,16 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
 }
 
 // Waits for the round enqueued with buffer set `buf` and checks it; returns
-// its overflow count in *rescored.
-sw_status wait_round(sw_ctx* ctx, sw_serve_state* s, int buf, uint64_t* rescored) {
+// its overflow count in *rescored and its device time in *device_ms (from its
+// table upload to its last copy: the stream reaches the round's first
+// operation only when the round before has ended, so rounds do not overlap).
+sw_status wait_round(sw_ctx* ctx, sw_serve_state* s, int buf, uint64_t* rescored,
+                     double* device_ms) {
     SW_CUDA(ctx, cudaEventSynchronize(s->done_ev[buf]));
     SW_CUDA(ctx, cudaGetLastError());
+    float ms = 0.f;
+    SW_CUDA(ctx, cudaEventElapsedTime(&ms, s->start_ev[buf], s->done_ev[buf]));
+    *device_ms = ms;
     const int flagged = *s->h_flagged[buf];
     if ((size_t)flagged > s->ovf_cap)
         SW_SET(ctx, SW_ERR_UNSUPPORTED, "%d overflow entries exceed the list (%zu)", flagged,
@@ -610,6 +629,7 @@ void run_solo(sw_ctx* ctx, sw_serve_state* s, std::vector<Request>& reqs) {
         s->stats.launches += ctx->stats.launches;
         s->stats.rescored += ctx->stats.rescored;
         s->stats.busy_ms += t1 - t0;
+        s->stats.device_ms += ctx->stats.kernel_ms;
         if (st == SW_OK) {
             r.hits.assign(hits.begin(), hits.begin() + nh);
             s->stats.cells += (uint64_t)r.query.size() * ctx->n_residues;
@@ -691,11 +711,13 @@ void scheduler(sw_ctx* ctx) {
     // in flight fails (the slots' score rows are no longer trustworthy)
     auto complete = [&](InFlight& r) {
         uint64_t rescored = 0;
-        const sw_status st = wait_round(ctx, s, r.buf, &rescored);
+        double device_ms = 0;
+        const sw_status st = wait_round(ctx, s, r.buf, &rescored, &device_ms);
         const double t1 = now_ms();
         {
             std::lock_guard<std::mutex> lock(s->mu);
             s->stats.rescored += rescored;
+            s->stats.device_ms += device_ms;
             s->stats.busy_ms += t1 - std::max(r.t_enq, last_done);
             last_done = t1;
             hand_out(ctx, s, r, st, t1);
@@ -842,6 +864,7 @@ extern "C" void sw_serve_options_default(sw_serve_options* o) {
     o->pair_group_width = 16;
     o->pair_rows_per_thread = 64;
     o->pair_long = 1;
+    o->pair_regions = 0;
 }
 
 extern "C" sw_status sw_serve_start(sw_ctx* ctx, const sw_serve_options* opt) {
@@ -856,6 +879,7 @@ extern "C" sw_status sw_serve_start(sw_ctx* ctx, const sw_serve_options* opt) {
     const QpKernel* qk = o.pair_rows > 0 ? find_qp(o.pair_group_width, o.pair_rows_per_thread)
                                          : nullptr;
     if (!k || o.max_active == 0 || o.chunks == 0 || o.stack_rows < 0 || o.pair_rows < 0 ||
+        o.pair_regions < 0 ||
         (o.pair_rows > 0 && !qk))
         SW_SET(ctx, SW_ERR_INVALID, "bad serving options");
     // the tallest stack the shape holds (whole passes whose profile fits one
@@ -923,11 +947,15 @@ extern "C" sw_status sw_serve_start(sw_ctx* ctx, const sw_serve_options* opt) {
     ids.reserve((size_t)npairs);
     s->chunk_begin.assign(1, 0);
     for (int c = 0; c < s->n_chunks; ++c) {
+        uint64_t cols = 0;
         for (int64_t p = c; p < npairs; p += s->n_chunks) {
             ring.push_back(host_pairs[(size_t)p]);
             ids.push_back((uint32_t)p);
+            s->ring_ncols.push_back(host_pairs[(size_t)p].ncols);
+            cols += host_pairs[(size_t)p].ncols;
         }
         s->chunk_begin.push_back((int)ring.size());
+        s->chunk_cols.push_back(cols);
     }
     if (dev_alloc(&s->d_pairs, ring.size()) != cudaSuccess ||
         dev_alloc(&s->d_pair_ids, ids.size()) != cudaSuccess)
@@ -938,7 +966,7 @@ extern "C" sw_status sw_serve_start(sw_ctx* ctx, const sw_serve_options* opt) {
          cudaMemcpy(s->d_pair_ids, ids.data(), ids.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess))
         return fail("pair ring");
     if (dev_alloc(&s->d_scores, (size_t)s->n_slots * std::max(n_rec, 1)) != cudaSuccess ||
-        dev_alloc(&s->d_counters, 4 * (size_t)s->n_slots + 8) != cudaSuccess)
+        dev_alloc(&s->d_counters, 6 * (size_t)s->n_slots + 16) != cudaSuccess)
         return fail("slots");
     // overflow entries: one per (request, record) at worst, bounded
     s->ovf_cap = std::min<size_t>((size_t)s->n_slots * std::max(n_rec, 1),
@@ -954,14 +982,17 @@ extern "C" sw_status sw_serve_start(sw_ctx* ctx, const sw_serve_options* opt) {
                                       (qk->block / qk->T));
     if (dev_alloc(&s->d_bnd, groups * s->bnd_group) != cudaSuccess) return fail("boundary rows");
     if (qk && o.pair_long) {
-        // up to 4 boundary regions (copies of the per-record rows, 8 bytes per
-        // column of every record) so that tall double stacks' segments share
-        // launches, as many as fit in an eighth of the free memory
+        // boundary regions (copies of the per-record rows, 8 bytes per column
+        // of every record) so that tall double stacks' segments share
+        // launches: pair_regions of them (0: up to 16), as many as fit in an
+        // eighth of the free memory.  Few regions split the tall stacks into
+        // waves of short launches, and each launch ends in a tail where the
+        // last long records finish on a few SMs.
         const size_t stride = (size_t)ctx->db_units * 16;
         size_t fb = 0, tb = 0;
         if (cudaMemGetInfo(&fb, &tb) != cudaSuccess) cudaGetLastError();
         const size_t fit = stride ? fb / 8 / (stride * sizeof(uint2)) : 0;
-        const int n = (int)std::min<size_t>(4, fit);
+        const int n = (int)std::min<size_t>(o.pair_regions > 0 ? (size_t)o.pair_regions : 16, fit);
         if (n > 1 && dev_alloc(&s->d_segbnd, (size_t)n * stride) == cudaSuccess) {
             s->seg_regions = n;
             s->seg_stride = stride;
@@ -976,13 +1007,15 @@ extern "C" sw_status sw_serve_start(sw_ctx* ctx, const sw_serve_options* opt) {
                 cudaSuccess ||
             cudaMallocHost((void**)&s->h_flagged[b], sizeof(int)) != cudaSuccess)
             return fail("pinned keys");
-        if (cudaEventCreateWithFlags(&s->done_ev[b], cudaEventDisableTiming) != cudaSuccess)
+        if (cudaEventCreate(&s->done_ev[b]) != cudaSuccess ||
+            cudaEventCreate(&s->start_ev[b]) != cudaSuccess)
             return fail("round events");
     }
-    // stacks (at most one per slot), the overflow count, and paired entries
-    // (a lane of at most max_stack_rows rows has at most that / pair_seg
-    // segments; two lanes per double stack)
-    s->counters_cap = 4 * (size_t)s->n_slots + 8;
+    // stacks (at most one per slot), the overflow count, paired entries (a
+    // lane of at most max_stack_rows rows has at most that / pair_seg
+    // segments; two lanes per double stack) and one long-phase counter per
+    // paired launch (at most one per entry, plus one)
+    s->counters_cap = 6 * (size_t)s->n_slots + 16;
     s->slots.assign((size_t)s->n_slots, Slot());
     s->stats.slots = (uint32_t)s->n_slots;
     s->stats.chunks = (uint32_t)s->n_chunks;
