@@ -711,6 +711,16 @@ def run_ours(args, rank, world, local_rank):
                 "peak_source": "measured live: libswprobe paired-query cell mix"}
             line["batched"] = batched
         if served is not None:
+            # the rounds run the same paired kernel: rate over the rounds'
+            # device time against the same measured mix
+            pm = rates.get("cell_pair_mix_gcups")
+            dg = served["saturated"].get("device_gcups")
+            served["roofline"] = {
+                "bound": "int_alu (packed int16x2 DPX, paired queries)",
+                "achieved": dg, "peak": round(pm, 1) if pm else None, "unit": "GCUPS",
+                "frac": round(dg / pm, 4) if pm and dg else None,
+                "peak_source": "measured live: libswprobe paired-query cell mix; achieved = "
+                               "saturated cells / the rounds' device time (CUDA events)"}
             line["served"] = served
         if stress is not None:
             line["stress"] = stress

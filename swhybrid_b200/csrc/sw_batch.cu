@@ -47,8 +47,7 @@ struct BatchLaunch {
     int counter_base;          // first counter of this launch
     bool long_part;            // runs on the side stream
     size_t bnd_group;
-    int long_units = 0;        // paired: units of the long phase (QpArgs::long_units) ...
-    int long_ordinal = 0;      // ... and its counter, after the entries' counters
+    int long_units = 0;        // paired: units of the long phase (QpArgs::long_units)
 };
 
 // Host image of a batch's stacks (uploaded as one block, see enqueue_batch).
@@ -252,10 +251,8 @@ sw_status enqueue_batch(sw_ctx* ctx, sw_batch_state* b, uint32_t nq, size_t qbyt
     SW_CUDA(ctx, cudaMemcpyAsync(b->d_meta, b->h_stage + meta_at, ml.total,
                                  cudaMemcpyHostToDevice, st));
     const int nst = ml.nst;
-    int n_qp_launches = 0;
-    for (const BatchLaunch& L : launches) n_qp_launches += L.qk ? 1 : 0;
-    SW_CUDA(ctx, cudaMemsetAsync(b->d_counters, 0,
-                                 (2 * (size_t)nst + 1 + ml.nqp + n_qp_launches) * sizeof(int), st));
+    SW_CUDA(ctx, cudaMemsetAsync(b->d_counters, 0, (2 * (size_t)nst + 1 + ml.nqp) * sizeof(int),
+                                 st));
     SW_CUDA(ctx, cudaMemsetAsync(b->d_scores, 0, (size_t)nq * n_rec * sizeof(int), st));
     const uint32_t* d_qoff = reinterpret_cast<const uint32_t*>(b->d_meta + ml.qoff);
     const uint32_t* d_qlen = reinterpret_cast<const uint32_t*>(b->d_meta + ml.qlen);
@@ -302,7 +299,6 @@ sw_status enqueue_batch(sw_ctx* ctx, sw_batch_state* b, uint32_t nq, size_t qbyt
             q.seg_slot = reinterpret_cast<const uint32_t*>(b->d_meta + ml.qp_slot) + L.sbegin;
             q.seg_stride = b->seg_stride;
             q.long_units = L.long_units;
-            q.long_counter = b->d_counters + 2 * nst + 1 + ml.nqp + L.long_ordinal;
             void* args[] = {&q};
             SW_CUDA(ctx, cudaLaunchKernel(L.qk->fn, dim3((unsigned)L.grid), dim3(L.threads), args,
                                           L.smem, st));
@@ -546,7 +542,6 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
     StackPlan sp;
     std::vector<BatchLaunch> launches;
     size_t bnd_long = 0, bnd_bulk = 0;
-    int n_qp_launches = 0;
     int nst_total = 0;
     for (const Bucket& bk : buckets) nst_total += (int)bk.stacks.size();
     int sidx = 0;
@@ -741,14 +736,12 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
                 [&](int p) { return (uint64_t)ctx->pair_ncols[(size_t)p]; },
                 (int)ctx->n_pairs, ctx->pair_cols_total,
                 (long long)L.grid * (L.threads / qk->T));
-            L.long_ordinal = n_qp_launches++;
             bnd_bulk = std::max(bnd_bulk, (size_t)L.grid * (L.threads / qk->T) * L.bnd_group);
             launches.push_back(L);
         }
     }
     // counters: bulk of stack i at [i], long at [nst_total + i], overflow count
-    // at [2 nst_total], paired double stack j at [2 nst_total + 1 + j], the
-    // long phase of paired launch l at [2 nst_total + 1 + nqp + l]
+    // at [2 nst_total], paired double stack j at [2 nst_total + 1 + j]
     const MetaLayout ml = meta_layout(nq, sp);
 
     // ---- buffers (before any capture) ----
@@ -761,7 +754,7 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
         }
         b->graphs.clear();
     };
-    const size_t counters_need = 2 * (size_t)nst_total + 1 + ml.nqp + n_qp_launches;
+    const size_t counters_need = 2 * (size_t)nst_total + 1 + ml.nqp;
     if (std::max<uint64_t>(qbytes, 1) > b->queries_cap || ml.total > b->meta_cap ||
         counters_need > b->counters_cap)
         drop_graphs();

@@ -175,6 +175,7 @@ extern "C" sw_status sw_ctx_create(int device, const sw_params* params, sw_ctx**
         return st;
     }
     auto fail = [&](sw_status s) {
+        cudaGetLastError();     // a refused call must not surface in the caller's next one
         sw_ctx_destroy(ctx);
         return s;
     };
@@ -208,29 +209,24 @@ extern "C" sw_status sw_ctx_create(int device, const sw_params* params, sw_ctx**
     if (cudaMemcpy(ctx->d_mat, mat8, 1024, cudaMemcpyHostToDevice) != cudaSuccess)
         return fail(SW_ERR_CUDA);
     if (dev_alloc(&ctx->d_counters, 16) != cudaSuccess) return fail(SW_ERR_NOMEM);
-    // every first-pass shape may use the opt-in shared-memory maximum
+    // every first-pass kernel may use the opt-in shared-memory maximum, less
+    // what it holds statically (the long-pair kernels hold a few words)
+    auto allow_smem = [&](const void* fn) {
+        cudaFuncAttributes fa;
+        return cudaFuncGetAttributes(&fa, fn) == cudaSuccess &&
+               cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    ctx->max_smem - (int)fa.sharedSizeBytes) == cudaSuccess;
+    };
     int nk = 0;
     const WfKernel* ks = wf_kernels(&nk);
     for (int i = 0; i < nk; ++i)
-        if (cudaFuncSetAttribute(ks[i].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 ctx->max_smem) != cudaSuccess ||
-            cudaFuncSetAttribute(ks[i].batch_fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 ctx->max_smem) != cudaSuccess)
-            return fail(SW_ERR_CUDA);
+        if (!allow_smem(ks[i].fn) || !allow_smem(ks[i].batch_fn)) return fail(SW_ERR_CUDA);
     const QpKernel* qks = qp_kernels(&nk);
     for (int i = 0; i < nk; ++i)
-        if (cudaFuncSetAttribute(qks[i].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 ctx->max_smem) != cudaSuccess)
-            return fail(SW_ERR_CUDA);
-    // the long-pair kernels also hold a few static shared words
+        if (!allow_smem(qks[i].fn)) return fail(SW_ERR_CUDA);
     const LongKernel* lks = long_kernels(&nk);
-    for (int i = 0; i < nk; ++i) {
-        cudaFuncAttributes fa;
-        if (cudaFuncGetAttributes(&fa, lks[i].fn) != cudaSuccess ||
-            cudaFuncSetAttribute(lks[i].fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 ctx->max_smem - (int)fa.sharedSizeBytes) != cudaSuccess)
-            return fail(SW_ERR_CUDA);
-    }
+    for (int i = 0; i < nk; ++i)
+        if (!allow_smem(lks[i].fn)) return fail(SW_ERR_CUDA);
     *out = ctx;
     return SW_OK;
 }

@@ -66,10 +66,9 @@ struct QpArgs {
     size_t seg_stride;
     // units [0, long_units) are the launch's long records (longest first):
     // they are scored before the rest, in items of one unit per group of a
-    // block, all from one double stack (long_counter: items claimed, zero
-    // before), so no block holds its groups at a stack's end for one long unit
+    // block, all from one double stack, so that no block holds its groups at
+    // a stack's end for one long unit
     int long_units;
-    int* long_counter;
 };
 
 // Host planning of paired lanes (batched search and serving).  Items (queries)
@@ -550,14 +549,16 @@ __device__ __forceinline__ void run_qpairs(const QpArgs& a, const uint4* prof, i
 #undef SWQ_SET_SEG
 }
 
-// The paired-query batched kernel.  First the long units: a block claims
-// items of G = BLOCK / T consecutive long units of one double stack (similar
-// lengths, the pair table being longest first), one per group; then the
-// blocks walk the double stacks in order, claiming the other units.
+// The paired-query batched kernel.  First the long units: items of G = BLOCK
+// / T consecutive long units of one double stack (similar lengths, the pair
+// table being longest first), one per group, dealt to the blocks round-robin
+// (block b takes items b, b + gridDim.x, ...; a block left with less long
+// work starts the rest earlier); then the blocks walk the double stacks in
+// order, claiming the other units.  The kernel holds no static shared memory
+// (the host gives the dynamic profile the whole opt-in maximum).
 template <int T, int R, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, 1) sw_qpbatch(const QpArgs a) {
     extern __shared__ uint4 prof4[];
-    __shared__ int s_item;
     constexpr int G = BLOCK / T;
     const int units = 2 * a.pair_count;
     const int n_long = min(a.long_units, units);
@@ -576,12 +577,8 @@ __global__ void __launch_bounds__(BLOCK, 1) sw_qpbatch(const QpArgs a) {
     if (n_long > 0) {
         const int per = (n_long + G - 1) / G;
         const int items = per * a.nstacks;
-        while (true) {
-            __syncthreads();    // the previous item is done and s_item was read
-            if (threadIdx.x == 0) s_item = atomicAdd(a.long_counter, 1);
-            __syncthreads();
-            const int it = s_item;
-            if (it >= items) break;
+        for (int it = (int)blockIdx.x; it < items; it += (int)gridDim.x) {
+            __syncthreads();    // every group is done with the previous item
             const int i = it / per;
             const int u = (it - i * per) * G + (int)threadIdx.x / T;
             const int P = stage(i);

@@ -413,8 +413,8 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
             SW_CUDA(ctx, cudaMemsetAsync(s->d_scores + (size_t)sl * n_rec, 0,
                                          (size_t)n_rec * sizeof(int), st));
     // counters: stack i at [i], the overflow count at [ns], paired entry j at
-    // [ns + 1 + j], the long phase of paired launch l at [ns + 1 + ne + l]
-    const size_t n_counters = ns + 1 + ne + qp_launches.size();
+    // [ns + 1 + j]
+    const size_t n_counters = ns + 1 + ne;
     if (n_counters > s->counters_cap)
         SW_SET(ctx, SW_ERR_UNSUPPORTED, "%zu paired launch entries exceed the counters (%zu)", ne,
                s->counters_cap);
@@ -425,7 +425,6 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
                T, R);
     int* d_ovf_count = s->d_counters + ns;
     const int pair_count = s->chunk_begin[chunk + 1] - s->chunk_begin[chunk];
-    size_t qp_ordinal = 0;
     for (const QpLaunch& L : pair_count > 0 ? qp_launches : std::vector<QpLaunch>()) {
         const size_t smem = qk->smem((int)std::max<uint32_t>(L.max_rows, 1));
         int occq = 0;
@@ -480,7 +479,6 @@ sw_status enqueue_round(sw_ctx* ctx, sw_serve_state* s, int chunk, int buf,
         q.long_units = qp_long_units([&](int p) { return (uint64_t)s->ring_ncols[(size_t)(cb + p)]; },
                                      pair_count, s->chunk_cols[(size_t)chunk],
                                      (long long)occq * ctx->num_sms * (qk->block / qk->T));
-        q.long_counter = s->d_counters + ns + 1 + ne + qp_ordinal++;
         void* qargs[] = {&q};
         SW_CUDA(ctx, cudaLaunchKernel(qk->fn, dim3((unsigned)(occq * ctx->num_sms)),
                                       dim3(qk->block), qargs, smem, st));
@@ -1011,10 +1009,9 @@ extern "C" sw_status sw_serve_start(sw_ctx* ctx, const sw_serve_options* opt) {
             cudaEventCreate(&s->start_ev[b]) != cudaSuccess)
             return fail("round events");
     }
-    // stacks (at most one per slot), the overflow count, paired entries (a
-    // lane of at most max_stack_rows rows has at most that / pair_seg
-    // segments; two lanes per double stack) and one long-phase counter per
-    // paired launch (at most one per entry, plus one)
+    // stacks (at most one per slot), the overflow count, and paired entries
+    // (a lane of at most max_stack_rows rows has at most that / pair_seg
+    // segments; two lanes per double stack)
     s->counters_cap = 6 * (size_t)s->n_slots + 16;
     s->slots.assign((size_t)s->n_slots, Slot());
     s->stats.slots = (uint32_t)s->n_slots;
