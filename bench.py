@@ -56,6 +56,8 @@ WORKLOADS = {
     "traceback": "profiling case: the full-size DB, one query of 1,434 and the alignments of its "
                  "top-10 hits (sw_traceback) per step",
     "probe": "the roofline probe alone: register-only cell mixes and issue rates (libswprobe.so)",
+    "serve": "profiling case: the full-size DB and --serve-requests requests (lengths log-uniform "
+             "30..8,000) queued at once on sw_serve_* (the serving leg's saturated phase)",
 }
 
 
@@ -78,6 +80,8 @@ def parse(argv=None):
                     help="requests per offered load in the serving leg (0 = skip it)")
     ap.add_argument("--serve-levels", type=str, default="0.25,0.5,0.75,1.0",
                     help="offered loads of the serving leg, as fractions of the saturating rate")
+    ap.add_argument("--serve-half-requests", type=int, default=1000,
+                    help="requests at the 50%% offered load (p99 at half load)")
     ap.add_argument("--serve-chunks", type=int, default=None,
                     help="serving: DB chunks of the ring (default: the library's)")
     ap.add_argument("--serve-slots", type=int, default=None,
@@ -317,12 +321,21 @@ def run_reference(args, rank, world):
 
 
 # ---------------------------------------------------------------------------
-def serve_leg(ctx, db, n_req: int, seed: int = 5, loads=(0.25, 0.5, 0.75, 1.0), opts=None):
+def serve_options(args) -> dict:
+    """The serving options given on the command line (others: the library's)."""
+    return {k: v for k, v in (("chunks", args.serve_chunks), ("max_active", args.serve_slots),
+                              ("pair_long", args.serve_pair_long),
+                              ("pair_regions", args.serve_regions)) if v is not None}
+
+
+def serve_leg(ctx, db, n_req: int, seed: int = 5, loads=(0.25, 0.5, 0.75, 1.0), opts=None,
+              n_half: int = 0):
     """Serving: requests of lengths log-uniform 30..8,000 (seeded) against the
     resident DB through sw_serve_*.  First the saturating rate (3x the slot
     count submitted at once), then Poisson arrivals at 25/50/75/100% of it,
-    n_req requests each; every request's top-10 is checked against the plain
-    path for a seeded subset."""
+    n_req requests each (n_half at 50%, when larger: the first n_req of them
+    are the other levels' requests); a seeded subset of every level's top-10
+    lists is checked against the plain path."""
     from swhybrid_b200 import capi, synth as _synth
     rng = np.random.default_rng(seed)
 
@@ -354,10 +367,11 @@ def serve_leg(ctx, db, n_req: int, seed: int = 5, loads=(0.25, 0.5, 0.75, 1.0), 
         levels = []
         check_ids = []
         base = 1_000_000
-        level_qs = requests(n_req)           # the same requests at every offered load
+        level_qs = requests(max(n_req, n_half))   # the same requests at every offered load
         for frac in loads:
-            qs = level_qs
-            arr = _synth.poisson_arrivals(rng, n_req, frac * sat_rate)
+            n_l = max(n_req, n_half) if frac == 0.5 else n_req
+            qs = level_qs[:n_l]
+            arr = _synth.poisson_arrivals(rng, n_l, frac * sat_rate)
             st0 = ctx.serve_stats()
             t_start = time.perf_counter()
             for i, (q, ta) in enumerate(zip(qs, arr)):
@@ -365,7 +379,7 @@ def serve_leg(ctx, db, n_req: int, seed: int = 5, loads=(0.25, 0.5, 0.75, 1.0), 
                 if delay > 0:
                     time.sleep(delay)
                 ctx.serve_submit(base + i, q)
-            got_l = collect(n_req, 600)
+            got_l = collect(n_l, 600)
             st1 = ctx.serve_stats()
             lat = np.array([r["done_ms"] - r["submit_ms"] for r in got_l.values()])
             wait = np.array([r["start_ms"] - r["submit_ms"] for r in got_l.values()])
@@ -375,7 +389,7 @@ def serve_leg(ctx, db, n_req: int, seed: int = 5, loads=(0.25, 0.5, 0.75, 1.0), 
             levels.append({
                 "offered_fraction": frac,
                 "offered_rate_per_s": round(frac * sat_rate, 3),
-                "requests": n_req, "completed": len(got_l),
+                "requests": n_l, "completed": len(got_l),
                 "ok": int(sum(1 for r in got_l.values() if r["status"] == 0)),
                 "latency_ms_p50": round(float(np.percentile(lat, 50)), 1),
                 "latency_ms_p99": round(float(np.percentile(lat, 99)), 1),
@@ -386,7 +400,7 @@ def serve_leg(ctx, db, n_req: int, seed: int = 5, loads=(0.25, 0.5, 0.75, 1.0), 
                 "rounds": int(st1.rounds - st0.rounds),
                 "launches": int(st1.launches - st0.launches),
             })
-            sel = rng.choice(n_req, size=min(8, n_req), replace=False)
+            sel = rng.choice(n_l, size=min(8, n_l), replace=False)
             check_ids += [(qs[i], got_l.get(base + i)) for i in sel]
             base += 1_000_000
         st = ctx.serve_stats()
@@ -397,8 +411,10 @@ def serve_leg(ctx, db, n_req: int, seed: int = 5, loads=(0.25, 0.5, 0.75, 1.0), 
     return {
         "workload": "requests of lengths log-uniform 30..8,000 (seeded) against the full-size DB; "
                     "saturating rate from %d requests queued at once, then Poisson arrivals at "
-                    "%s%% of it, the same %d requests at every level" % (
-                        3 * slots, "/".join(f"{100 * f:g}" for f in loads), n_req),
+                    "%s%% of it, the same %d requests at every level%s" % (
+                        3 * slots, "/".join(f"{100 * f:g}" for f in loads), n_req,
+                        " (%d at 50%%, the first %d of them the same)" % (n_half, n_req)
+                        if n_half > n_req and 0.5 in loads else ""),
         "slots": slots, "chunks": int(st.chunks),
         "saturated": {"requests": len(sat_q), "rate_per_s": round(sat_rate, 3),
                       "gcups": round(sat_cells / ((t1 - t0) * 1e-3) / 1e9, 1),
@@ -618,11 +634,7 @@ def run_ours(args, rank, world, local_rank):
         ctx.set_stream(None)
         served = serve_leg(ctx, db, args.serve_requests,
                            loads=tuple(float(x) for x in args.serve_levels.split(",") if x),
-                           opts={k: v for k, v in (("chunks", args.serve_chunks),
-                                                   ("max_active", args.serve_slots),
-                                                   ("pair_long", args.serve_pair_long),
-                                                   ("pair_regions", args.serve_regions))
-                                 if v is not None})
+                           opts=serve_options(args), n_half=args.serve_half_requests)
 
     # ---- overflow / long-record stress (its own DB and context) ----
     stress = None
@@ -798,10 +810,12 @@ def run_shard(args, rank, world, local_rank, make_ctx=None, workload=None):
 
 
 def run_case(args, local_rank):
-    """Profiling cases (--workload batched | traceback): one call of the
-    batched search or of the traceback of a query's hits per step.  Batched:
-    device time by CUDA events inside the library; traceback: host wall time
-    (sw_traceback keeps no device timings).  Prints one JSON line."""
+    """Profiling cases (--workload batched | traceback | serve): one call of
+    the batched search or of the traceback of a query's hits per step, or the
+    serving leg's saturated phase once.  Batched: device time by CUDA events
+    inside the library; traceback: host wall time (sw_traceback keeps no
+    device timings); serve: the rounds' device time (sw_serve_stats) and wall
+    time.  Prints one JSON line."""
     import torch
     from swhybrid_b200 import autotune, capi, synth
     torch.cuda.set_device(local_rank)
@@ -810,6 +824,32 @@ def run_case(args, local_rank):
     try:
         ctx.load_db(db.residues, db.offsets)
         autotune.apply(ctx)
+        if args.workload == "serve":
+            rng = np.random.default_rng(5)
+            qs = [synth.residues(rng, int(L))
+                  for L in synth.loguniform_lengths(rng, args.serve_requests, 30, 8000)]
+            ctx.serve_start(**serve_options(args))
+            try:
+                t0 = capi.serve_clock_ms()
+                for i, q in enumerate(qs):
+                    ctx.serve_submit(i, q)
+                got = {}
+                while len(got) < len(qs):
+                    for r in ctx.serve_poll(256, timeout_ms=200):
+                        got[r["id"]] = r
+                t1 = max(r["done_ms"] for r in got.values())
+                st = ctx.serve_stats()
+            finally:
+                ctx.serve_stop()
+            cells = sum(len(q) for q in qs) * db.total
+            print(json.dumps({"workload": WORKLOADS[args.workload], "requests": len(qs),
+                              "slots": int(st.slots), "chunks": int(st.chunks),
+                              "ok": sum(1 for r in got.values() if r["status"] == 0),
+                              "wall_ms": round(t1 - t0, 1), "device_ms": round(st.device_ms, 1),
+                              "gcups": round(cells / ((t1 - t0) * 1e-3) / 1e9, 1),
+                              "rounds": int(st.rounds), "launches": int(st.launches)}),
+                  flush=True)
+            return
         batched = args.workload == "batched"
         if batched:
             if args.no_pairs:        # every query in stacks (the stacked kernel alone)
@@ -846,7 +886,7 @@ def run_case(args, local_rank):
 
 def main(argv=None):
     args = parse(argv)
-    if args.workload in ("batched", "traceback"):
+    if args.workload in ("batched", "traceback", "serve"):
         run_case(args, int(os.environ.get("LOCAL_RANK", "0")))
         return 0
     if args.workload == "probe":
