@@ -49,6 +49,34 @@ struct LongBlock {
     static constexpr int value = R <= 8 ? 768 : R <= 16 ? 512 : R <= 32 ? 384 : 256;
 };
 
+// One column step of a warp's two half-columns (top on column c with profile
+// words t0/t1, bottom on column c - 1 with b0/b1); f_bot receives the bottom
+// half's last-row F.  Both halves' maxima go into S.
+template <int R>
+__device__ __forceinline__ void long_step(uint32_t (&H)[R], uint32_t (&E)[R], const uint2* t0,
+                                          const uint2* t1, const uint2* b0, const uint2* b1,
+                                          uint32_t prev_h, uint32_t f_in, uint32_t& mid_h,
+                                          uint32_t& mid_f, uint32_t& f_bot_out, uint32_t& S,
+                                          const CellK& K) {
+    constexpr int HALF = R / 2;
+    constexpr int JSTRIDE = kCodes * GroupShape<kLT>::SLOTS;
+    const uint32_t bot_diag = mid_h;
+    uint32_t f_top = f_in, f_bot = mid_f;
+    mid_h = H[HALF - 1];
+    reverse_sweep<R, 0, HALF>(H, E, t0, t1, JSTRIDE, prev_h);
+    reverse_sweep<R, HALF, R>(H, E, b0, b1, JSTRIDE, bot_diag);
+#pragma unroll
+    for (int i = 0; i < HALF; ++i) {
+        forward_cell(H[i], E[i], f_top, K);
+        forward_cell(H[HALF + i], E[HALF + i], f_bot, K);
+        if (i & 1) S = __vimax3_s16x2(S, H[i - 1], H[i]);
+        if (i & 1) S = __vimax3_s16x2(S, H[HALF + i - 1], H[HALF + i]);
+        if (!(i & 1) && i == HALF - 1) S = __vimax3_s16x2(S, H[i], H[HALF + i]);
+    }
+    mid_f = f_top;
+    f_bot_out = f_bot;
+}
+
 template <int R>
 __global__ void __launch_bounds__(LongBlock<R>::value, 1) sw_long(const LongArgs a) {
     constexpr int T = kLT;
@@ -119,9 +147,54 @@ __global__ void __launch_bounds__(LongBlock<R>::value, 1) sw_long(const LongArgs
     SWL_BEGIN_PAIR(s_next[g], 0)
     int gs = 0;                                            // block step
     while (true) {
-        for (int j = 0; j < kLK; ++j, ++gs) {
+        for (int j = 0; j < kLK;) {
             const int s = gs - start - w * kLD;            // this warp's step (warp-uniform)
-            if (!active || s < 0 || s >= span) continue;
+            if (!active || s < 0 || s >= span) {
+                ++j;
+                ++gs;
+                continue;
+            }
+            // Plain steps: every lane's two half-columns and its next residue
+            // lie inside the pair (column s - 2t - 1 >= 0 for t = 31, column
+            // s + 1 < ncols for t = 0), so the warp runs them with no bounds
+            // guards, up to the next barrier.
+            if (s >= 2 * T - 1 && s <= ncols - 2) {
+                int n = ncols - 1 - s;
+                if (n > kLK - j) n = kLK - j;
+                const int ct0 = s - 2 * t;
+                const bool ring_rd = t == 0 && w > 0;
+                const bool ring_wr = t == T - 1 && w + 1 < P;
+#pragma unroll 2
+                for (int i = 0; i < n; ++i) {
+                    uint32_t h_in = __shfl_up_sync(FULL, out_h, 1);
+                    uint32_t f_in = __shfl_up_sync(FULL, out_f, 1);
+                    const uint32_t d_in = d_cur;
+                    const int ct = ct0 + i;
+                    d_cur = (uint32_t)__ldg(col + ct + 1);
+                    if (t == 0) {
+                        h_in = Z;
+                        f_in = Z;
+                    }
+                    if (ring_rd) {
+                        const uint2 b = ring_in[(s + i) & (kLRing - 1)];
+                        h_in = b.x;
+                        f_in = b.y;
+                    }
+                    long_step<R>(H, E, prof_p + (int)(d_in & 0xffu) * SLOTS,
+                                 prof_p + (int)((d_in >> 8) & 0xffu) * SLOTS,
+                                 prof_p + (int)(d_bot & 0xffu) * SLOTS,
+                                 prof_p + (int)((d_bot >> 8) & 0xffu) * SLOTS, prev_h, f_in,
+                                 mid_h, mid_f, out_f, S, K);
+                    out_h = H[R - 1];
+                    if (ring_wr) ring_out[(ct - 1) & (kLRing - 1)] = make_uint2(out_h, out_f);
+                    prev_h = h_in;
+                    d_bot = d_in;
+                }
+                j += n;
+                gs += n;
+                continue;
+            }
+            // a general step: lanes at the pair's first or last columns
             uint32_t h_in = __shfl_up_sync(FULL, out_h, 1);
             uint32_t f_in = __shfl_up_sync(FULL, out_f, 1);
             const uint32_t d_in = d_cur;       // this thread's top column, loaded a step ahead
@@ -146,24 +219,12 @@ __global__ void __launch_bounds__(LongBlock<R>::value, 1) sw_long(const LongArgs
             if (ct >= 0 && ct <= ncols) {
                 const uint32_t wt = top_valid ? d_in : kPadPair;
                 const uint32_t wb = bot_valid ? d_bot : kPadPair;
-                const uint2* t0 = prof_p + (int)(wt & 0xffu) * SLOTS;
-                const uint2* t1 = prof_p + (int)((wt >> 8) & 0xffu) * SLOTS;
-                const uint2* b0 = prof_p + (int)(wb & 0xffu) * SLOTS;
-                const uint2* b1 = prof_p + (int)((wb >> 8) & 0xffu) * SLOTS;
-                const uint32_t bot_diag = mid_h;
-                uint32_t f_top = f_in, f_bot = mid_f;
-                mid_h = H[HALF - 1];
-                reverse_sweep<R, 0, HALF>(H, E, t0, t1, JSTRIDE, prev_h);
-                reverse_sweep<R, HALF, R>(H, E, b0, b1, JSTRIDE, bot_diag);
-#pragma unroll
-                for (int i = 0; i < HALF; ++i) {
-                    forward_cell(H[i], E[i], f_top, K);
-                    forward_cell(H[HALF + i], E[HALF + i], f_bot, K);
-                    if (i & 1) S = __vimax3_s16x2(S, H[i - 1], H[i]);
-                    if (i & 1) S = __vimax3_s16x2(S, H[HALF + i - 1], H[HALF + i]);
-                    if (!(i & 1) && i == HALF - 1) S = __vimax3_s16x2(S, H[i], H[HALF + i]);
-                }
-                mid_f = f_top;
+                uint32_t f_bot = Z;
+                long_step<R>(H, E, prof_p + (int)(wt & 0xffu) * SLOTS,
+                             prof_p + (int)((wt >> 8) & 0xffu) * SLOTS,
+                             prof_p + (int)(wb & 0xffu) * SLOTS,
+                             prof_p + (int)((wb >> 8) & 0xffu) * SLOTS, prev_h, f_in, mid_h,
+                             mid_f, f_bot, S, K);
                 if (bot_valid) {
                     out_h = H[R - 1];
                     out_f = f_bot;
@@ -173,6 +234,8 @@ __global__ void __launch_bounds__(LongBlock<R>::value, 1) sw_long(const LongArgs
             }
             prev_h = h_in;
             d_bot = d_in;
+            ++j;
+            ++gs;
         }
         // barrier: pipelines whose pair ends here publish their passes' maxima
         // and (leader) claim the next pair; the OR says whether any pipeline
