@@ -97,6 +97,30 @@ def test_cutover_split_bit_exact(ctx):
         ctx.set_kernel_config(None)
 
 
+def test_long_pairs_near_the_plain_step_bounds(ctx):
+    """The long-pair kernel runs unguarded column steps only while every lane
+    of a warp is inside its pair (steps 63 .. ncols - 2); pairs of 40..140
+    columns (those above 60 in the long kernel) put the first and last plain
+    steps at every offset from a barrier, with one to three pipelined passes,
+    against the oracle."""
+    rng = np.random.default_rng(43)
+    lens = rng.integers(40, 141, size=600)
+    db = synth.db_from_lengths(rng, lens)
+    qs = [synth.residues(rng, L) for L in (200, 700)]
+    db, _ = synth.plant_homologs(rng, db, qs[1], 0.03)
+    wants = [oracle.search(q, db.residues, db.offsets, M, 12, 2) for q in qs]
+    ctx.load_db(db.residues, db.offsets)
+    try:
+        for rows in (8, 16, 24):
+            for q, want in zip(qs, wants):
+                ctx.set_kernel_config((32, rows, 8, 12, 60))
+                _, scores = ctx.search(q, want_scores=True)
+                np.testing.assert_array_equal(scores, want, err_msg=f"R={rows} qlen={len(q)}")
+                assert ctx.run_stats().long_ms > 0
+    finally:
+        ctx.set_kernel_config(None)
+
+
 def test_streamed_segments_short_and_empty_records(ctx):
     """The plain kernel's groups stream from pass to pass and pair to pair
     without draining the wavefront.  Records of 0..80 residues (pairs shorter
