@@ -98,7 +98,8 @@ typedef struct sw_run_stats {
     uint64_t rescored;      /* records re-scored by the 32-bit pass */
     uint32_t launches;      /* kernels this library launched in the last call */
     uint32_t queries;
-    sw_kernel_config used;  /* shape of the last plain search */
+    sw_kernel_config used;  /* shape of the last plain search (with a row-segment
+                               plan: its first segment's shape as the short one) */
     double long_ms;         /* last plain search with a cut-over: long-pair launch time */
     double bulk_ms;         /* ... and the concurrent bulk launch time (else 0, 0) */
 } sw_run_stats;
@@ -247,26 +248,62 @@ sw_status sw_search_device(struct sw_ctx *ctx, const uint8_t *d_query,
 /* Overrides the kernel shape chosen for plain searches (NULL = automatic). */
 sw_status sw_set_kernel_config(struct sw_ctx *ctx, const sw_kernel_config *cfg);
 
+/* One step of a row-segment plan: whole passes of group_width x
+ * rows_per_thread query rows.  In a tuning entry, passes = 0 means "the rest
+ * of the query" (its last pass padded); group_width = 0 ends the plan. */
+typedef struct sw_plan_step {
+    int32_t group_width;
+    int32_t rows_per_thread;
+    int32_t passes;
+} sw_plan_step;
+
+#define SW_PLAN_STEPS 4
+
 /* Shape table from the autotuner: for a query of qlen residues the first
  * entry (in the given order, sorted by max_qlen) with qlen <= max_qlen is used
  * when its shapes fit that length (else the cost model chooses).  A new
  * context starts with the table measured on B200 that is compiled into the
  * library (swhybrid_b200/tuned/b200.json); this call replaces it, and n = 0
- * clears it (the cost model alone chooses). */
+ * clears it (the cost model alone chooses).
+ *
+ * plan (optional, plan[0].group_width = 0 for none): the query's rows in
+ * consecutive row segments of different shapes, so that only the last
+ * segment's last pass holds padding rows.  Each step with passes > 0 takes
+ * exactly that many whole passes; the first step with passes = 0 (or, if
+ * none, the shape cfg gives the bulk launch) takes the rest.  Each segment
+ * reads the boundary row the one before it wrote, and scores merge by
+ * maximum, as when a query too long for one block's profile is split.  cfg
+ * still decides the long-pair cut-over; the plan covers the other pairs.
+ * The plan is not used (cfg's shape runs the whole query) when a shape
+ * override is set, when its fixed steps need more rows than the query has,
+ * when a segment's profile does not fit one pass of shared memory, or when a
+ * segment's shape would make its launch wait on one long record (the longest
+ * record pair it scores has more columns than a group's even share of the
+ * DB: such a shape only pays with the long-pair split).  sw_get_plan reports
+ * what a length runs. */
 typedef struct sw_tuning_entry {
     uint32_t max_qlen;
     sw_kernel_config cfg;
+    sw_plan_step plan[SW_PLAN_STEPS];
 } sw_tuning_entry;
 
 sw_status sw_set_tuning(struct sw_ctx *ctx, const sw_tuning_entry *entries, uint32_t n);
 
 /* The compiled kernel shapes: fills up to capacity (group width, rows per
- * thread) entries; *n_shapes receives the total. */
-sw_status sw_get_shapes(int32_t *group_width, int32_t *rows_per_thread, uint32_t capacity,
-                        uint32_t *n_shapes);
+ * thread, threads per block) entries (any array may be NULL); *n_shapes
+ * receives the total. */
+sw_status sw_get_shapes(int32_t *group_width, int32_t *rows_per_thread,
+                        int32_t *threads_per_block, uint32_t capacity, uint32_t *n_shapes);
 
 /* Shape the library would pick for a query of this length. */
 sw_status sw_get_kernel_config(struct sw_ctx *ctx, uint32_t qlen, sw_kernel_config *cfg);
+
+/* Row segments a plain search of this length runs on the DB's pairs below the
+ * long-pair cut-over, in order: each step's shape and passes (the last step
+ * holds the rest of the query, its last pass padded).  Fills up to capacity
+ * steps; *n_steps receives the count (1 without a plan). */
+sw_status sw_get_plan(struct sw_ctx *ctx, uint32_t qlen, sw_plan_step *steps, uint32_t capacity,
+                      uint32_t *n_steps);
 
 sw_status sw_get_run_stats(const struct sw_ctx *ctx, sw_run_stats *out);
 

@@ -122,14 +122,79 @@ def predict_gcups(results, shape: str, qlen: int) -> float | None:
     return None if r is None else r * qlen / rows_used(T, R, qlen)
 
 
-def table_from_sweep(results, step: int = 8, top: int = 8192) -> list:
-    """[(max_qlen, (T, R, T, R, cutover)), ...]: the shape with the best
+def plan_shapes(results, blocks: dict) -> list:
+    """Shapes a row-segment plan may use: at most 16 groups (record pairs in
+    flight) per block.  On the 205 M-residue DB an evenly loaded group of
+    such a shape gets more columns than the longest record pair (35,000), so
+    its launch does not end on one pair's serial column steps; a narrower
+    shape only pays with the long-pair split, which a plan does not use.  The
+    library checks the same rule against the DB at hand and runs the single
+    shape instead when a plan breaks it."""
+    shapes = sorted({s for L in results for s in results[L]["all"]})
+    out = []
+    for s in shapes:
+        T, R = (int(x) for x in s.split("x"))
+        b = blocks.get((T, R))
+        if b is not None and b // T <= 16:
+            out.append(s)
+    return out
+
+
+def best_plans(results, shapes, step: int = 8, top: int = 8192, max_steps: int = 4) -> dict:
+    """{q: (predicted time, [(T, R, passes), ...])} for q on the grid: the
+    fastest predicted row-segment plan of at most max_steps steps from
+    `shapes`, each step whole passes but the last (passes 0: the rest of the
+    query, its last pass padded).  Time is in rows / GCUPS units: a step of
+    P whole passes costs P*T*R / predict_gcups(shape, P*T*R), the rest
+    L / predict_gcups(shape, L).  Whole passes are multiples of 8 rows
+    (T >= 4, R even), so every remainder is again a grid point."""
+    memo = {}
+
+    def g(s, rows):
+        key = (s, rows)
+        if key not in memo:
+            memo[key] = predict_gcups(results, s, rows)
+        return memo[key]
+
+    best = {}
+    for q in range(step, top + step, step):
+        bt, bp = float("inf"), None
+        for s in shapes:
+            v = g(s, q)
+            if v and q / v < bt:
+                T, R = (int(x) for x in s.split("x"))
+                bt, bp = q / v, [(T, R, 0)]
+        for s in shapes:
+            T, R = (int(x) for x in s.split("x"))
+            for P in range(1, (q - 1) // (T * R) + 1):
+                rows = P * T * R
+                v = g(s, rows)
+                rest = best.get(q - rows)
+                if not v or rest is None or rest[1] is None or len(rest[1]) >= max_steps:
+                    continue
+                t = rows / v + rest[0]
+                if t < bt:
+                    bt, bp = t, [(T, R, P)] + rest[1]
+        best[q] = (bt, bp)
+    return best
+
+
+def table_from_sweep(results, step: int = 8, top: int = 8192, blocks: dict | None = None,
+                     plan_margin: float = 0.02) -> list:
+    """[(max_qlen, (T, R, T, R, cutover), plan), ...]: the shape with the best
     predicted GCUPS (predict_gcups) on a grid of query lengths, runs of equal
     choices merged.  The cut-over is the one measured with that shape at the
     nearest measured length when the shape was the best there, else 0 (the
-    library's automatic rule)."""
+    library's automatic rule).  plan: the fastest predicted row-segment plan
+    (best_plans over plan_shapes) when it beats that shape by more than
+    plan_margin and has at least two steps (whole passes of one shape, then
+    the rest with another, so only the last pass holds padding rows), else
+    ().  blocks: threads per block by shape (default: the library's)."""
     Ls = sorted(results)
     shapes = sorted({s for L in Ls for s in results[L]["all"]})
+    if blocks is None:
+        blocks = capi.shape_blocks()
+    plans = best_plans(results, plan_shapes(results, blocks), step, top)
     out = []
     for q in range(step, top + step, step):
         best, bg = None, -1.0
@@ -143,20 +208,25 @@ def table_from_sweep(results, step: int = 8, top: int = 8192) -> list:
         cut = int(results[near].get("cutover", 0)) if results[near]["best"] == best else 0
         T, R = (int(x) for x in best.split("x"))
         cfg = (T, R, T, R, cut)
-        if out and out[-1][1] == cfg:
-            out[-1] = (q, cfg)
+        plan = ()
+        pt, pp = plans.get(q, (float("inf"), None))
+        if pp is not None and len(pp) >= 2 and pt * (1.0 + plan_margin) < q / bg:
+            plan = tuple(pp)
+        if out and out[-1][1] == cfg and out[-1][2] == plan:
+            out[-1] = (q, cfg, plan)
         else:
-            out.append((q, cfg))
+            out.append((q, cfg, plan))
     if out:
         T, R = (int(x) for x in results[Ls[-1]]["best"].split("x"))
-        out.append((1 << 30, (T, R, T, R, int(results[Ls[-1]].get("cutover", 0)))))
+        out.append((1 << 30, (T, R, T, R, int(results[Ls[-1]].get("cutover", 0))), ()))
     return out
 
 
 def save(results, path: str = DEFAULT_TABLE, meta=None):
     os.makedirs(os.path.dirname(path), exist_ok=True)
     doc = {"meta": meta or {}, "sweep": {str(k): v for k, v in results.items()},
-           "table": [[hi, list(cfg)] for hi, cfg in table_from_sweep(results)]}
+           "table": [[hi, list(cfg)] + ([[list(st) for st in plan]] if plan else [])
+                     for hi, cfg, plan in table_from_sweep(results)]}
     with open(path, "w") as f:
         json.dump(doc, f, indent=1)
 
@@ -166,7 +236,9 @@ def load_table(path: str = DEFAULT_TABLE):
         return None
     with open(path) as f:
         doc = json.load(f)
-    return [(int(hi), tuple(int(x) for x in cfg)) for hi, cfg in doc["table"]]
+    return [(int(row[0]), tuple(int(x) for x in row[1]),
+             tuple(tuple(int(x) for x in st) for st in row[2]) if len(row) > 2 else ())
+            for row in doc["table"]]
 
 
 def apply(ctx: capi.Context, path: str = DEFAULT_TABLE) -> bool:

@@ -31,11 +31,17 @@ def default_header_text(table_path: str = TABLE) -> str:
         "",
         "namespace swb {",
         "",
-        "// {max_qlen, {long T, long R, short T, short R, cut-over}}",
+        "// {max_qlen, {long T, long R, short T, short R, cut-over}[, row-segment plan:",
+        "//  {{T, R, passes}, ...}, passes 0 = the rest of the query]}",
         "constexpr sw_tuning_entry kDefaultTuning[] = {",
     ]
-    for hi, cfg in doc["table"]:
-        lines.append("    {%du, {%d, %d, %d, %d, %d}}," % (int(hi), *(int(x) for x in cfg)))
+    for row in doc["table"]:
+        hi, cfg = row[0], row[1]
+        text = "    {%du, {%d, %d, %d, %d, %d}" % (int(hi), *(int(x) for x in cfg))
+        if len(row) > 2 and row[2]:
+            text += ", {" + ", ".join("{%d, %d, %d}" % tuple(int(x) for x in st)
+                                      for st in row[2]) + "}"
+        lines.append(text + "},")
     lines += ["};", "", "}  // namespace swb", ""]
     return "\n".join(lines)
 

@@ -27,7 +27,7 @@ SW_FLAG_REFERENCE_CAP = 1
 EXPORTS = [
     "sw_params_default", "sw_encode", "sw_ctx_create", "sw_ctx_destroy",
     "sw_last_error", "sw_db_load", "sw_db_stats_get", "sw_search",
-    "sw_search_device", "sw_set_kernel_config", "sw_get_kernel_config",
+    "sw_search_device", "sw_set_kernel_config", "sw_get_kernel_config", "sw_get_plan",
     "sw_get_run_stats", "sw_set_stream", "sw_sync", "sw_reset_totals", "sw_get_totals",
     "sw_set_tuning", "sw_score_noalloc", "sw_get_shapes", "sw_set_batch_options",
     "sw_search_batch", "sw_serve_options_default", "sw_serve_start", "sw_serve_submit",
@@ -114,8 +114,17 @@ class sw_serve_stats(ctypes.Structure):
                 ("pending", ctypes.c_uint32), ("device_ms", ctypes.c_double)]
 
 
+class sw_plan_step(ctypes.Structure):
+    _fields_ = [("group_width", ctypes.c_int32), ("rows_per_thread", ctypes.c_int32),
+                ("passes", ctypes.c_int32)]
+
+
+PLAN_STEPS = 4     # SW_PLAN_STEPS
+
+
 class sw_tuning_entry(ctypes.Structure):
-    _fields_ = [("max_qlen", ctypes.c_uint32), ("cfg", sw_kernel_config)]
+    _fields_ = [("max_qlen", ctypes.c_uint32), ("cfg", sw_kernel_config),
+                ("plan", sw_plan_step * PLAN_STEPS)]
 
 
 class sw_db_stats(ctypes.Structure):
@@ -199,7 +208,11 @@ def load(path: str | None = None):
                                   ctypes.POINTER(ctypes.c_uint32), P]
     L.sw_get_shapes.restype = ctypes.c_int
     L.sw_get_shapes.argtypes = [ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
-                                ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]
+                                ctypes.POINTER(ctypes.c_int32), ctypes.c_uint32,
+                                ctypes.POINTER(ctypes.c_uint32)]
+    L.sw_get_plan.restype = ctypes.c_int
+    L.sw_get_plan.argtypes = [P, ctypes.c_uint32, ctypes.POINTER(sw_plan_step), ctypes.c_uint32,
+                              ctypes.POINTER(ctypes.c_uint32)]
     L.sw_score_noalloc.restype = ctypes.c_int
     L.sw_score_noalloc.argtypes = [ctypes.c_int, ctypes.POINTER(sw_params), ctypes.c_void_p,
                                    ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
@@ -326,11 +339,23 @@ def shapes() -> list:
     """Compiled (group width, rows per thread) shapes."""
     L = load()
     n = ctypes.c_uint32(0)
-    L.sw_get_shapes(None, None, 0, ctypes.byref(n))
+    L.sw_get_shapes(None, None, None, 0, ctypes.byref(n))
     T = (ctypes.c_int32 * n.value)()
     R = (ctypes.c_int32 * n.value)()
-    L.sw_get_shapes(T, R, n.value, ctypes.byref(n))
+    L.sw_get_shapes(T, R, None, n.value, ctypes.byref(n))
     return [(T[i], R[i]) for i in range(n.value)]
+
+
+def shape_blocks() -> dict:
+    """Threads per block of every compiled shape: {(group width, rows): threads}."""
+    L = load()
+    n = ctypes.c_uint32(0)
+    L.sw_get_shapes(None, None, None, 0, ctypes.byref(n))
+    T = (ctypes.c_int32 * n.value)()
+    R = (ctypes.c_int32 * n.value)()
+    B = (ctypes.c_int32 * n.value)()
+    L.sw_get_shapes(T, R, B, n.value, ctypes.byref(n))
+    return {(T[i], R[i]): B[i] for i in range(n.value)}
 
 
 def score_noalloc(device: int, params: sw_params, d_query: int, qlen: int, d_residues: int,
@@ -455,12 +480,29 @@ class Context:
         return out, (scores[:, :self.n_records] if want_scores else None)
 
     def set_tuning(self, table):
-        """table: [(max_qlen, (T, R, T, R, cutover)), ...] sorted by max_qlen."""
+        """table: [(max_qlen, (T, R, T, R, cutover)[, plan]), ...] sorted by
+        max_qlen; plan: up to PLAN_STEPS (T, R, passes) row-segment steps
+        (passes 0: the rest of the query)."""
         arr = (sw_tuning_entry * max(len(table), 1))()
-        for i, (hi, cfg) in enumerate(table):
+        for i, row in enumerate(table):
+            hi, cfg = row[0], row[1]
+            plan = row[2] if len(row) > 2 else ()
+            if len(plan) > PLAN_STEPS:
+                raise ValueError(f"plan of {len(plan)} steps (at most {PLAN_STEPS})")
             arr[i].max_qlen = int(hi)
             arr[i].cfg = sw_kernel_config(*cfg)
+            for j, (T, R, passes) in enumerate(plan):
+                arr[i].plan[j] = sw_plan_step(int(T), int(R), int(passes))
         self._check(self.L.sw_set_tuning(self.h, arr, len(table)), "sw_set_tuning")
+
+    def plan(self, qlen: int) -> list:
+        """Row segments a plain search of qlen runs: [(T, R, passes), ...]."""
+        steps = (sw_plan_step * (PLAN_STEPS + 1))()
+        n = ctypes.c_uint32(0)
+        self._check(self.L.sw_get_plan(self.h, qlen, steps, PLAN_STEPS + 1, ctypes.byref(n)),
+                    "sw_get_plan")
+        return [(steps[i].group_width, steps[i].rows_per_thread, steps[i].passes)
+                for i in range(n.value)]
 
     def kernel_config(self, qlen: int) -> tuple:
         c = sw_kernel_config()

@@ -488,16 +488,24 @@ double shape_cost(sw_ctx* ctx, const WfKernel& k, int qlen, int64_t b, int64_t e
     return work / (g_width * g_warps);
 }
 
-sw_kernel_config choose_config(sw_ctx* ctx, int qlen) {
-    if (ctx->has_override) return ctx->override_cfg;
+// The shape-table entry for a query length whose shapes fit it, or null (no
+// table, no entry, a shape override, or the entry's shapes do not fit).
+const sw_tuning_entry* find_entry(sw_ctx* ctx, int qlen) {
+    if (ctx->has_override) return nullptr;
     for (const sw_tuning_entry& e : ctx->tuning) {
         if ((uint32_t)qlen > e.max_qlen) continue;
         const WfKernel* kl = find_kernel(e.cfg.long_group_width, e.cfg.long_rows_per_thread);
         const WfKernel* ks = find_kernel(e.cfg.short_group_width, e.cfg.short_rows_per_thread);
         if (kl && ks && shape_occupancy(ctx, *kl, qlen) > 0 && shape_occupancy(ctx, *ks, qlen) > 0)
-            return e.cfg;
-        break;   // the tuned shape does not fit this length: fall back to the model
+            return &e;
+        return nullptr;   // the tuned shape does not fit this length: the model chooses
     }
+    return nullptr;
+}
+
+sw_kernel_config choose_config(sw_ctx* ctx, int qlen) {
+    if (ctx->has_override) return ctx->override_cfg;
+    if (const sw_tuning_entry* e = find_entry(ctx, qlen)) return e->cfg;
     int n = 0;
     const WfKernel* ks = wf_kernels(&n);
     const int64_t np = ctx->n_pairs;
@@ -534,10 +542,18 @@ extern "C" sw_status sw_set_kernel_config(sw_ctx* ctx, const sw_kernel_config* c
 extern "C" sw_status sw_set_tuning(sw_ctx* ctx, const sw_tuning_entry* entries, uint32_t n) {
     if (!ctx || (n && !entries)) return SW_ERR_INVALID;
     std::vector<sw_tuning_entry> tab(entries, entries + n);
-    for (const sw_tuning_entry& e : tab)
+    for (const sw_tuning_entry& e : tab) {
         if (!find_kernel(e.cfg.long_group_width, e.cfg.long_rows_per_thread) ||
             !find_kernel(e.cfg.short_group_width, e.cfg.short_rows_per_thread) || e.cfg.cutover < 0)
             SW_SET(ctx, SW_ERR_INVALID, "tuning entry names an uncompiled shape");
+        for (const sw_plan_step& s : e.plan) {
+            if (s.group_width == 0) break;
+            if (!find_kernel(s.group_width, s.rows_per_thread) || s.passes < 0 ||
+                s.passes > (1 << 20))
+                SW_SET(ctx, SW_ERR_INVALID, "plan step %dx%d x %d passes: no such shape",
+                       s.group_width, s.rows_per_thread, s.passes);
+        }
+    }
     for (size_t i = 1; i < tab.size(); ++i)
         if (tab[i].max_qlen < tab[i - 1].max_qlen)
             SW_SET(ctx, SW_ERR_INVALID, "tuning entries not sorted by max_qlen");
@@ -552,8 +568,22 @@ extern "C" sw_status sw_get_kernel_config(sw_ctx* ctx, uint32_t qlen, sw_kernel_
     return SW_OK;
 }
 
+namespace swb {
+sw_status describe_plan(sw_ctx* ctx, int qlen, sw_plan_step* steps, uint32_t capacity,
+                        uint32_t* n_steps);
+}
+
+extern "C" sw_status sw_get_plan(sw_ctx* ctx, uint32_t qlen, sw_plan_step* steps,
+                                 uint32_t capacity, uint32_t* n_steps) {
+    if (!ctx || !n_steps || (capacity && !steps)) return SW_ERR_INVALID;
+    if (!ctx->db_loaded) SW_SET(ctx, SW_ERR_STATE, "no DB loaded");
+    if (qlen > (1u << 24)) SW_SET(ctx, SW_ERR_UNSUPPORTED, "query of %u residues", qlen);
+    return describe_plan(ctx, (int)std::max<uint32_t>(qlen, 1), steps, capacity, n_steps);
+}
+
 extern "C" sw_status sw_get_shapes(int32_t* group_width, int32_t* rows_per_thread,
-                                   uint32_t capacity, uint32_t* n_shapes) {
+                                   int32_t* threads_per_block, uint32_t capacity,
+                                   uint32_t* n_shapes) {
     if (!n_shapes) return SW_ERR_INVALID;
     int n = 0;
     const WfKernel* k = wf_kernels(&n);
@@ -561,6 +591,7 @@ extern "C" sw_status sw_get_shapes(int32_t* group_width, int32_t* rows_per_threa
     for (uint32_t i = 0; i < capacity && i < (uint32_t)n; ++i) {
         if (group_width) group_width[i] = k[i].T;
         if (rows_per_thread) rows_per_thread[i] = k[i].R;
+        if (threads_per_block) threads_per_block[i] = k[i].block;
     }
     return SW_OK;
 }
@@ -590,20 +621,74 @@ sw_status take_marks(sw_ctx* ctx, sw_ctx::Marks* m) {
     return SW_OK;
 }
 
+// A row segment of a plain search: the next `rows` query rows with shape k
+// (consecutive launches of whole passes when the profile of all of them does
+// not fit one block).
+struct RowSeg {
+    const WfKernel* k;
+    int rows;
+};
+constexpr int kMaxRowSegs = SW_PLAN_STEPS + 1;
+
 // Cut-over for a configuration without one: a DB whose longest pair needs more
 // column steps than an evenly loaded bulk group gets (the bulk launch would end
 // on a few serial chains: groups claim pairs longest first, so below that the
 // long pairs finish inside the share) sends the pairs above a quarter of the
 // share to the long-pair kernel; otherwise no split.
+// Columns of one pass over the DB that an evenly loaded group of shape k gets.
+double group_share(sw_ctx* ctx, const WfKernel& k, int qlen) {
+    const int occ = std::max(1, shape_occupancy(ctx, k, qlen));
+    const double groups = (double)occ * ctx->num_sms * (k.block / k.T);
+    return (double)ctx->pair_cols_total / groups;
+}
+
 int auto_cutover(sw_ctx* ctx, const sw_kernel_config& cfg, int qlen) {
     if (ctx->n_pairs == 0) return 0;
     const WfKernel* k = find_kernel(cfg.short_group_width, cfg.short_rows_per_thread);
     if (!k) return 0;
-    const int occ = std::max(1, shape_occupancy(ctx, *k, qlen));
-    const double groups = (double)occ * ctx->num_sms * (k->block / k->T);
-    const double share = (double)ctx->pair_cols_total / groups;
+    const double share = group_share(ctx, *k, qlen);
     if ((double)ctx->pair_ncols[0] <= share) return 0;
     return std::max(1024, (int)(share / 4));
+}
+
+// The row segments a plain search runs on the pairs [bulk_begin, n_pairs):
+// the table entry's plan when it applies, else the whole query with the bulk
+// shape ks (which also takes the rest of a plan without a rest step).  The
+// plan is dropped (one segment) when a step names an uncompiled shape, when
+// its fixed steps need more rows than the query has, when a segment's profile
+// does not fit one pass in shared memory, or when a segment's shape is narrow
+// enough that one group's even share of the columns is below the longest
+// pair's (its launch would end on that pair's serial column steps: narrow
+// shapes only pay with the long-pair split).
+int build_plan(sw_ctx* ctx, int qlen, const WfKernel* ks, int64_t bulk_begin, RowSeg* out) {
+    out[0] = RowSeg{ks, qlen};
+    const sw_tuning_entry* e = find_entry(ctx, qlen);
+    if (!e || e->plan[0].group_width == 0 || !ks || bulk_begin >= ctx->n_pairs) return 1;
+    RowSeg segs[kMaxRowSegs];
+    int n = 0, left = qlen;
+    for (int i = 0; i < SW_PLAN_STEPS && left > 0; ++i) {
+        const sw_plan_step& s = e->plan[i];
+        if (s.group_width == 0) break;
+        const WfKernel* k = find_kernel(s.group_width, s.rows_per_thread);
+        if (!k || s.passes < 0) return 1;
+        if (s.passes == 0) {
+            segs[n++] = RowSeg{k, left};
+            left = 0;
+            break;
+        }
+        const int64_t rows = (int64_t)s.passes * k->T * k->R;
+        if (rows > left) return 1;
+        segs[n++] = RowSeg{k, (int)rows};
+        left -= (int)rows;
+    }
+    if (left > 0) segs[n++] = RowSeg{ks, left};
+    const double longest = (double)ctx->pair_ncols[bulk_begin];
+    for (int i = 0; i < n; ++i)
+        if (launch_rows(ctx, *segs[i].k, segs[i].rows) == 0 ||
+            longest > group_share(ctx, *segs[i].k, segs[i].rows))
+            return 1;
+    std::copy(segs, segs + n, out);
+    return n;
 }
 
 // The long-pair kernel for a query: the configured long shape when the
@@ -656,6 +741,39 @@ const LongKernel* choose_long(sw_ctx* ctx, const sw_kernel_config& cfg, int qlen
     return nullptr;
 }
 
+// sw_get_plan: the bulk range and row segments enqueue_search would run (its
+// cut-over rule: the long-pair kernel takes the pairs above the cut-over when
+// some, but not all, pairs are, and a pipelined shape fits the length; else
+// one shape, the long one without a cut-over, takes every pair).
+sw_status describe_plan(sw_ctx* ctx, int qlen, sw_plan_step* steps, uint32_t capacity,
+                        uint32_t* n_steps) {
+    const sw_kernel_config cfg = choose_config(ctx, qlen);
+    const int cutover = cfg.cutover > 0 ? cfg.cutover : auto_cutover(ctx, cfg, qlen);
+    int64_t n_long = ctx->n_pairs, bulk_b = 0;
+    if (cutover > 0) {
+        n_long = 0;
+        while (n_long < ctx->n_pairs && (int)ctx->pair_ncols[n_long] > cutover) ++n_long;
+    }
+    int T = cfg.long_group_width, R = cfg.long_rows_per_thread;
+    if (n_long < ctx->n_pairs) {
+        T = cfg.short_group_width;
+        R = cfg.short_rows_per_thread;
+        int lp = 0, lg = 0;
+        size_t ls = 0;
+        if (n_long > 0 && choose_long(ctx, cfg, qlen, &lp, &lg, &ls)) bulk_b = n_long;
+    }
+    const WfKernel* k = find_kernel(T, R);
+    if (!k) SW_SET(ctx, SW_ERR_INVALID, "no kernel %dx%d", T, R);
+    RowSeg plan[kMaxRowSegs];
+    const int n = build_plan(ctx, qlen, k, bulk_b, plan);
+    *n_steps = (uint32_t)n;
+    for (int i = 0; i < n && (uint32_t)i < capacity; ++i) {
+        const int rp = plan[i].k->T * plan[i].k->R;
+        steps[i] = sw_plan_step{plan[i].k->T, plan[i].k->R, (plan[i].rows + rp - 1) / rp};
+    }
+    return SW_OK;
+}
+
 sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t* d_scores_rec,
                          unsigned long long** keys_final, uint32_t* launches) {
     cudaStream_t st = ctx->stream;
@@ -697,17 +815,25 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
             ctx->stats.used.long_rows_per_thread = lk->R;
         }
     }
+    // the bulk launches: the pairs the long-pair kernel does not take, in
+    // the row segments of the length's plan
+    const Seg& bulk = split ? segs[1] : (segs[0].e > segs[0].b ? segs[0] : segs[1]);
+    RowSeg plan[kMaxRowSegs];
+    int nplan = 0;
     // every shape is checked before anything is launched: a search refused
     // half-way would leave a launch in flight that writes into the next one
-    for (int si = split ? 1 : 0; si < 2; ++si) {
-        const Seg& sg = segs[si];
-        if (sg.e <= sg.b) continue;
-        const WfKernel* k = find_kernel(sg.T, sg.R);
-        if (!k) SW_SET(ctx, SW_ERR_INVALID, "no kernel %dx%d", sg.T, sg.R);
+    if (bulk.e > bulk.b) {
+        const WfKernel* k = find_kernel(bulk.T, bulk.R);
+        if (!k) SW_SET(ctx, SW_ERR_INVALID, "no kernel %dx%d", bulk.T, bulk.R);
         if (launch_rows(ctx, *k, qlen) == 0)
             SW_SET(ctx, SW_ERR_UNSUPPORTED,
                    "one pass of shape %dx%d does not fit shared memory (profile %zu bytes)",
-                   sg.T, sg.R, k->smem(sg.T * sg.R));
+                   bulk.T, bulk.R, k->smem(bulk.T * bulk.R));
+        nplan = build_plan(ctx, qlen, k, bulk.b, plan);
+        if (nplan > 1) {
+            ctx->stats.used.short_group_width = plan[0].k->T;
+            ctx->stats.used.short_rows_per_thread = plan[0].k->R;
+        }
     }
     // the search's timing events, taken after every check (a refused search
     // holds none), then its buffers cleared
@@ -769,39 +895,36 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
         SW_CUDA(ctx, cudaEventRecord(mk.e[6], st));
     }
     mk.split = split;
-    for (int si = split ? 1 : 0; si < 2; ++si) {
-        const Seg& sg = segs[si];
-        if (sg.e <= sg.b) continue;
-        const WfKernel* k = find_kernel(sg.T, sg.R);
-        if (!k) SW_SET(ctx, SW_ERR_INVALID, "no kernel %dx%d", sg.T, sg.R);
-        // rows per launch: the whole query, or row segments of whole passes
-        // scored by consecutive launches (boundary row handed on, scores
-        // merged by maximum)
-        const int seg_rows = launch_rows(ctx, *k, qlen);
-        if (seg_rows == 0)
-            SW_SET(ctx, SW_ERR_UNSUPPORTED,
-                   "one pass of shape %dx%d does not fit shared memory (profile %zu bytes)",
-                   sg.T, sg.R, k->smem(sg.T * sg.R));
-        for (int r0 = 0; r0 < qlen; r0 += seg_rows) {
-            const int rows = std::min(seg_rows, qlen - r0);
+    // Row segments of the plan (one for most lengths), each in launches of
+    // whole passes up to what one block's profile holds: every launch but the
+    // first reads the boundary row the one before wrote (pass0 counts the
+    // query's passes before it, whatever their shapes: the row holds one
+    // 8-byte (H, F) entry per column and parity of the pass index, so its
+    // layout does not depend on the shape), and scores merge by maximum.
+    int r0 = 0, passes_before = 0;
+    for (int pi = 0; pi < nplan; ++pi) {
+        const WfKernel* k = plan[pi].k;
+        const int seg_rows = launch_rows(ctx, *k, plan[pi].rows);
+        for (int s0 = 0; s0 < plan[pi].rows; s0 += seg_rows) {
+            const int rows = std::min(seg_rows, plan[pi].rows - s0);
             const int occ = shape_occupancy(ctx, *k, rows);
-            if (r0 > 0)   // the previous segment's launch has claimed every pair
-                SW_CUDA(ctx, cudaMemsetAsync(ctx->d_counters + sg.counter, 0, sizeof(int), st));
+            if (r0 > 0)   // the previous launch has claimed every pair
+                SW_CUDA(ctx, cudaMemsetAsync(ctx->d_counters + bulk.counter, 0, sizeof(int), st));
             WfArgs a;
             a.db = ctx->d_db;
             a.pairs = ctx->d_pairs;
-            a.pair_begin = (int)sg.b;
-            a.pair_count = (int)(sg.e - sg.b);
+            a.pair_begin = (int)bulk.b;
+            a.pair_count = (int)(bulk.e - bulk.b);
             a.query = d_query + r0;
             a.qlen = rows;
-            a.pass0 = r0 / (k->T * k->R);
+            a.pass0 = passes_before;
             a.more = r0 + rows < qlen ? 1 : 0;
             a.mat = ctx->d_mat;
             a.bias2 = (uint32_t)(ctx->params.gap_open + ctx->params.gap_extend);
             a.bias2 |= a.bias2 << 16;
             a.neg_e = (uint32_t)(uint16_t)(int16_t)(-ctx->params.gap_extend);
             a.neg_e |= a.neg_e << 16;
-            a.counter = ctx->d_counters + sg.counter;
+            a.counter = ctx->d_counters + bulk.counter;
             a.bnd = ctx->d_bnd;
             a.scores = ctx->d_scores;
             a.n_records = (int)ctx->n_records;
@@ -811,12 +934,14 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
             void* args[] = {&a};
             int64_t grid = (int64_t)occ * (ctx->num_sms - reserved_sms);
             const int64_t groups_per_block = k->block / k->T;
-            grid = std::min<int64_t>(grid, ((sg.e - sg.b) + groups_per_block - 1) / groups_per_block);
+            grid = std::min<int64_t>(grid, ((bulk.e - bulk.b) + groups_per_block - 1) / groups_per_block);
             grid = std::max<int64_t>(grid, 1);
             SW_CUDA(ctx, cudaLaunchKernel(k->fn, dim3((unsigned)grid), dim3(k->block), args,
                                           k->smem(rows), st));
             ++*launches;
             ++mk.fp_launches;
+            r0 += rows;
+            passes_before += (rows + k->T * k->R - 1) / (k->T * k->R);
         }
     }
     if (split) {

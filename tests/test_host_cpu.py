@@ -90,13 +90,13 @@ def test_tuning_table_accounts_for_pass_padding():
         for s in rate:
             assert abs(autotune.predict_gcups(res, s, L) - res[L]["all"][s]) < 1e-6
     tab = autotune.table_from_sweep(res)
-    pick = lambda q: next(cfg for hi, cfg in tab if q <= hi)[:2]
+    pick = lambda q: next(cfg for hi, cfg, _ in tab if q <= hi)[:2]
     assert pick(1792) == (32, 56)       # one full 1,792-row pass
     assert pick(1900) == (16, 64)       # 2 x 1,024 rows, not 2 x 1,792
     assert pick(3584) == (32, 56)
-    assert [hi for hi, _ in tab] == sorted(hi for hi, _ in tab)
+    assert [row[0] for row in tab] == sorted(row[0] for row in tab)
     committed = autotune.load_table()
-    assert committed and [hi for hi, _ in committed] == sorted(hi for hi, _ in committed)
+    assert committed and [row[0] for row in committed] == sorted(row[0] for row in committed)
     # every shape whose profile fits one block was measured at every length
     # (a shape that does not fit still runs, in row segments over several
     # launches, and the table never picks it where it does not fit)
@@ -107,11 +107,47 @@ def test_tuning_table_accounts_for_pass_padding():
             for R in autotune.ROWS:
                 if autotune.profile_fits(T, R, int(L)):
                     assert f"{T}x{R}" in v["all"], (L, T, R)
-    for hi, c in committed:
+    for hi, c, _ in committed:
         if hi < (1 << 30):
             assert autotune.profile_fits(c[2], c[3], hi), (hi, c)
     # the library's built-in table is the committed one
     from swhybrid_b200 import build
     assert open(build.DEFAULT_HEADER).read() == build.default_header_text()
     shapes = set(capi.shapes())
-    assert all((c[0], c[1]) in shapes and (c[2], c[3]) in shapes for _, c in committed)
+    assert all((c[0], c[1]) in shapes and (c[2], c[3]) in shapes for _, c, _ in committed)
+
+
+def test_tuning_table_row_segment_plans():
+    """Row-segment plans: with two shapes of known rates on the rows they
+    compute, a length that is one pass of each runs as those two segments
+    instead of padding either shape's last pass.  In the committed table every
+    plan has 2..4 steps of shapes with at most 16 groups per block, fixed
+    steps of whole passes that leave rows for the rest at every length of the
+    entry's range, and the rest last."""
+    from swhybrid_b200 import autotune
+    rate = {"16x64": 4000.0, "32x20": 3800.0}
+    res = {}
+    for L in (600, 1000, 1500, 2000, 3000):
+        row = {s: rate[s] * L / autotune.rows_used(*map(int, s.split("x")), L) for s in rate}
+        res[L] = {"best": max(row, key=row.get), "cutover": 0, "all": row}
+    blocks = {(16, 64): 256, (32, 20): 512}
+    tab = autotune.table_from_sweep(res, blocks=blocks)
+    plan = next(p for hi, _, p in tab if 1664 <= hi)
+    assert sorted(plan) == sorted([(16, 64, 1), (32, 20, 0)]) or \
+        sorted(plan) == sorted([(32, 20, 1), (16, 64, 0)])
+    assert next(p for hi, _, p in tab if 1024 <= hi) == ()      # one whole pass
+    # a shape with more than 16 groups per block is never a plan step
+    assert not any(p for _, _, p in autotune.table_from_sweep(res, blocks={(16, 64): 384,
+                                                                           (32, 20): 640}))
+    committed = autotune.load_table()
+    lib_blocks = capi.shape_blocks()
+    prev, n_plans = 0, 0
+    for hi, cfg, plan in committed:
+        if plan:
+            n_plans += 1
+            assert 2 <= len(plan) <= capi.PLAN_STEPS
+            assert all(P > 0 for _, _, P in plan[:-1]) and plan[-1][2] == 0
+            assert sum(P * T * R for T, R, P in plan[:-1]) <= prev
+            assert all(lib_blocks[(T, R)] // T <= 16 for T, R, _ in plan)
+        prev = hi
+    assert n_plans > 0
