@@ -628,9 +628,11 @@ def run_ours(args, rank, world, local_rank):
             "launches_per_batch": b_launches,
         }
 
-    # ---- serving: continuous batching under Poisson arrivals ----
+    # ---- serving: continuous batching under Poisson arrivals (one GPU: the
+    # serving and stress legs are single-GPU measurements, so a multi-GPU run
+    # holds its GPUs only for the sharded sweep and the batched leg) ----
     served = None
-    if args.workload == "full" and args.serve_requests > 0:
+    if args.workload == "full" and args.serve_requests > 0 and world == 1:
         ctx.set_stream(None)
         served = serve_leg(ctx, db, args.serve_requests,
                            loads=tuple(float(x) for x in args.serve_levels.split(",") if x),
@@ -638,7 +640,7 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- overflow / long-record stress (its own DB and context) ----
     stress = None
-    if args.workload == "full" and not args.no_stress:
+    if args.workload == "full" and not args.no_stress and world == 1:
         stress = stress_leg(local_rank, args.steps)
 
     # ---- correctness spot check on the resident DB (rank 0, cheap) ----

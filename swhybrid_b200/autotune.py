@@ -45,6 +45,15 @@ def time_shape(ctx: capi.Context, dq, qlen: int, cfg: tuple, reps: int = 2) -> f
     return t.cells / (t.first_pass_ms * 1e-3) / 1e9
 
 
+def reps_for(L: int, reps: int) -> int:
+    """Searches timed per shape at query length L: at least `reps`, and
+    enough that short queries (a few milliseconds per search on the full DB)
+    are timed over about as many cells as a 4,000-residue one.  With one
+    search per shape a sweep picked shapes 7..22 % slower than the committed
+    table's for the queries of 144..310 residues."""
+    return max(reps, -(-4000 // max(int(L), 1)))
+
+
 def sweep(ctx: capi.Context, lengths, shapes=None, reps: int = 2, log=print,
           cutovers=(1024, 2048, 4096, 8192, 16384)):
     import torch
@@ -54,15 +63,16 @@ def sweep(ctx: capi.Context, lengths, shapes=None, reps: int = 2, log=print,
         q = synth.query(9000 + int(L), int(L))
         dq = torch.from_numpy(q).cuda()
         row = {}
+        n = reps_for(int(L), reps)
         for T, R in shapes:
-            g = time_shape(ctx, dq, int(L), (T, R, T, R, 0), reps)
+            g = time_shape(ctx, dq, int(L), (T, R, T, R, 0), n)
             if g is not None:
                 row[f"{T}x{R}"] = round(g, 1)
         best = max(row, key=row.get)
         T, R = (int(x) for x in best.split("x"))
         cut = {}
         for c in cutovers:
-            g = time_shape(ctx, dq, int(L), (T, R, T, R, c), reps)
+            g = time_shape(ctx, dq, int(L), (T, R, T, R, c), n)
             if g is not None:
                 cut[c] = round(g, 1)
         best_cut = max(cut, key=cut.get) if cut else 0

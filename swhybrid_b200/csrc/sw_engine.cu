@@ -630,11 +630,6 @@ struct RowSeg {
 };
 constexpr int kMaxRowSegs = SW_PLAN_STEPS + 1;
 
-// Cut-over for a configuration without one: a DB whose longest pair needs more
-// column steps than an evenly loaded bulk group gets (the bulk launch would end
-// on a few serial chains: groups claim pairs longest first, so below that the
-// long pairs finish inside the share) sends the pairs above a quarter of the
-// share to the long-pair kernel; otherwise no split.
 // Columns of one pass over the DB that an evenly loaded group of shape k gets.
 double group_share(sw_ctx* ctx, const WfKernel& k, int qlen) {
     const int occ = std::max(1, shape_occupancy(ctx, k, qlen));
@@ -642,6 +637,11 @@ double group_share(sw_ctx* ctx, const WfKernel& k, int qlen) {
     return (double)ctx->pair_cols_total / groups;
 }
 
+// Cut-over for a configuration without one: a DB whose longest pair needs more
+// column steps than an evenly loaded bulk group gets (the bulk launch would end
+// on a few serial chains: groups claim pairs longest first, so below that the
+// long pairs finish inside the share) sends the pairs above a quarter of the
+// share to the long-pair kernel; otherwise no split.
 int auto_cutover(sw_ctx* ctx, const sw_kernel_config& cfg, int qlen) {
     if (ctx->n_pairs == 0) return 0;
     const WfKernel* k = find_kernel(cfg.short_group_width, cfg.short_rows_per_thread);

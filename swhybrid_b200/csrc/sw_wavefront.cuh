@@ -642,12 +642,14 @@ __device__ __forceinline__ void run_stream(const RunArgs& a, const uint2* prof) 
             const bool rd0 = t == 0 && a.pass0 + pass > 0;            // boundary row in
             const bool zin = (t == 0 && a.pass0 + pass == 0) || (STACKED && my_first);
             const bool wr = t == T - 1 && wlim > 0;                   // boundary row out
-            if constexpr (R >= 40) {
+            if constexpr (R >= 40 && !(R == 64 && (T == 8 || T == 16))) {
                 // With 40 rows or more per thread there are registers to hold the
                 // next step's profile words: they are loaded at the start of a step
                 // from residues already in registers, so no step waits for its
-                // profile (+1.4..2.6 % at 16x48 and 8x40; at 32x24 it measured
-                // 1.2..1.6 % slower, so fewer rows keep the loads in the step).
+                // profile (+1.4..2.6 % at 16x48 and 8x40, +0.6 % at 16x56; at 32x24
+                // it measured 1.2..1.6 % slower, so fewer rows keep the loads in the
+                // step, and so do 16x64 and 8x64, 2.3 % and 0.6 % faster without it
+                // at 249 registers, while 4x64 and 32x64 keep it: 0.7 % and 0.2 %).
                 if (k > 0) {
                     constexpr int NT = HalfChunks<0, HALF>::N, NB = HalfChunks<HALF, R>::N;
                     // this step's words (top: the residues of column c; bottom: the

@@ -98,6 +98,33 @@ def test_plan_dropped_when_one_pair_would_hold_a_launch(case):
     np.testing.assert_array_equal(scores, oracle.search(qq, res, off, M, 12, 2, mode=1))
 
 
+def test_plan_with_long_pair_split(case):
+    """Five records of 3,000 residues make the entry's shape split its long
+    pairs off to the long-pair kernel (which scores them against the whole
+    query, concurrently); the plan then runs on the other pairs, whose
+    longest is below every step's share.  Scores equal the oracle's."""
+    db, q = case
+    rng = np.random.default_rng(6)
+    longs = [synth.residues(rng, 3000) for _ in range(4)] + [q[200:3000].copy()]
+    res = np.concatenate([db.residues] + longs).astype(np.uint8)
+    lens = np.concatenate([db.lengths(), [len(x) for x in longs]])
+    off = np.zeros(len(lens) + 1, dtype=np.uint64)
+    off[1:] = np.cumsum(lens)
+    qq = q[:2400]
+    with capi.Context(0, capi.default_params(top_k=10)) as c:
+        c.load_db(res, off)
+        c.set_tuning(table(PLAN))
+        assert c.plan(2400) == [(16, 48, 1), (32, 20, 1), (16, 56, 2)]
+        hits, scores = c.search(qq, want_scores=True)
+        used = c.run_stats().used
+    assert used.cutover > 0 and used.long_group_width == 32      # the split ran
+    want = oracle.search(qq, res, off, M, 12, 2, mode=1)
+    np.testing.assert_array_equal(scores, want)
+    ws, wi = oracle.topk(want, 10)
+    assert hits == list(zip(ws.tolist(), wi.tolist()))
+    assert hits[0][1] == len(lens) - 1      # the record copied from the query
+
+
 def test_plan_steps_refused_when_not_compiled():
     with capi.Context(0) as c:
         with pytest.raises(capi.SwError) as e:
