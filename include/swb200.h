@@ -230,10 +230,12 @@ sw_status sw_db_title(const struct sw_ctx *ctx, uint64_t record, const char **ti
  * merge (src/ResultList.h:37-79, src/WorkerPool.cpp:99-105).
  * hits: top_k entries; *n_hits receives how many have score > 0.
  * scores: optional (NULL or n_records int32), every record's score in DB order.
- * Any query length: a query whose profile does not fit one block's shared
- * memory (over ~8,000 residues with the wide shapes) is scored in row
- * segments of whole passes by consecutive launches, each handing its last
- * row (H and F per column) to the next, with the scores merged by maximum. */
+ * Any query length up to 2^24 residues (SW_ERR_UNSUPPORTED beyond; the same
+ * bound holds for sw_search_device and each query of sw_search_batch): a
+ * query whose profile does not fit one block's shared memory (over ~8,000
+ * residues with the wide shapes) is scored in row segments of whole passes by
+ * consecutive launches, each handing its last row (H and F per column) to the
+ * next, with the scores merged by maximum. */
 sw_status sw_search(struct sw_ctx *ctx, const uint8_t *query, uint32_t qlen,
                     sw_hit *hits, uint32_t *n_hits, int32_t *scores);
 

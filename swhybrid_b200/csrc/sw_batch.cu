@@ -449,8 +449,12 @@ extern "C" sw_status sw_search_batch(sw_ctx* ctx, uint32_t nq, const uint8_t* qu
     const int n_rec = (int)ctx->n_records;
     if ((uint64_t)nq * (uint64_t)std::max(n_rec, 1) >= (1ull << 31))
         SW_SET(ctx, SW_ERR_UNSUPPORTED, "batch too large: %u queries x %d records", nq, n_rec);
-    for (uint32_t i = 0; i < nq; ++i)
+    for (uint32_t i = 0; i < nq; ++i) {
         if (qoffsets[i + 1] < qoffsets[i]) SW_SET(ctx, SW_ERR_INVALID, "query offsets not monotone");
+        if (qoffsets[i + 1] - qoffsets[i] > kMaxQueryResidues)
+            SW_SET(ctx, SW_ERR_UNSUPPORTED, "query %u: %llu residues (at most %u)", i,
+                   (unsigned long long)(qoffsets[i + 1] - qoffsets[i]), kMaxQueryResidues);
+    }
     const uint64_t qbytes = qoffsets[nq] - qoffsets[0];
     if (qbytes && !queries) SW_SET(ctx, SW_ERR_INVALID, "null queries");
     for (uint64_t i = 0; i < qbytes; ++i)

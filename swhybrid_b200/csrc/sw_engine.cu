@@ -577,7 +577,8 @@ extern "C" sw_status sw_get_plan(sw_ctx* ctx, uint32_t qlen, sw_plan_step* steps
                                  uint32_t capacity, uint32_t* n_steps) {
     if (!ctx || !n_steps || (capacity && !steps)) return SW_ERR_INVALID;
     if (!ctx->db_loaded) SW_SET(ctx, SW_ERR_STATE, "no DB loaded");
-    if (qlen > (1u << 24)) SW_SET(ctx, SW_ERR_UNSUPPORTED, "query of %u residues", qlen);
+    if (qlen > kMaxQueryResidues)
+        SW_SET(ctx, SW_ERR_UNSUPPORTED, "query of %u residues (at most %u)", qlen, kMaxQueryResidues);
     return describe_plan(ctx, (int)std::max<uint32_t>(qlen, 1), steps, capacity, n_steps);
 }
 
@@ -1073,6 +1074,8 @@ sw_status search_host(sw_ctx* ctx, const uint8_t* query, uint32_t qlen, sw_hit* 
     if (!ctx->db_loaded) SW_SET(ctx, SW_ERR_STATE, "no DB loaded (call sw_db_load first)");
     if ((qlen && !query) || (!hits && ctx->params.top_k > 0) || !n_hits)
         SW_SET(ctx, SW_ERR_INVALID, "null argument");
+    if (qlen > kMaxQueryResidues)
+        SW_SET(ctx, SW_ERR_UNSUPPORTED, "query of %u residues (at most %u)", qlen, kMaxQueryResidues);
     const double t0 = now_ms();
     const int k = ctx->params.top_k;
     for (int i = 0; i < k; ++i) hits[i] = sw_hit{0, 0, 0};
@@ -1136,6 +1139,8 @@ extern "C" sw_status sw_search_device(sw_ctx* ctx, const uint8_t* d_query, uint3
     if (ctx->serve) return SW_ERR_BUSY;   // the serving loop owns the stream and the DB
     if (!ctx->db_loaded) SW_SET(ctx, SW_ERR_STATE, "no DB loaded (call sw_db_load first)");
     if (!d_query || qlen == 0) SW_SET(ctx, SW_ERR_INVALID, "empty query");
+    if (qlen > kMaxQueryResidues)
+        SW_SET(ctx, SW_ERR_UNSUPPORTED, "query of %u residues (at most %u)", qlen, kMaxQueryResidues);
     SW_CUDA(ctx, cudaSetDevice(ctx->device));
     ctx->stats = sw_run_stats{};
     unsigned long long* keys = nullptr;

@@ -26,6 +26,10 @@
                    cudaGetErrorString(_e), __FILE__, __LINE__);             \
     } while (0)
 
+// Longest query any search entry point takes, in residues (16.7 M, far above
+// any protein; keeps row counts and offsets in 32-bit ints).
+constexpr uint32_t kMaxQueryResidues = 1u << 24;
+
 template <typename T>
 inline cudaError_t dev_alloc(T** p, size_t count) {
     *p = nullptr;

@@ -304,3 +304,27 @@ def test_bad_codes_rejected(ctx):
     with pytest.raises(capi.SwError) as e:
         ctx.search(bad)
     assert e.value.status == 1
+
+
+def test_query_longer_than_the_bound_refused(ctx):
+    """Queries of more than 2^24 residues are refused before any device work
+    (the plain, the resident and the batched entry points), and the context
+    keeps working."""
+    import torch
+    db = synth.small_db(2, 100)
+    ctx.load_db(db.residues, db.offsets)
+    big = np.zeros((1 << 24) + 1, dtype=np.uint8)
+    with pytest.raises(capi.SwError) as e:
+        ctx.search(big)
+    assert e.value.status == 6
+    d_big = torch.from_numpy(big).cuda()
+    with pytest.raises(capi.SwError) as e:
+        ctx.search_device(d_big.data_ptr(), big.size)
+    assert e.value.status == 6
+    with pytest.raises(capi.SwError) as e:
+        ctx.search_batch([synth.query(1, 50), big])
+    assert e.value.status == 6
+    q = synth.query(1, 50)
+    hits, scores = ctx.search(q, want_scores=True)
+    want = oracle.search(q, db.residues, db.offsets, M, 12, 2, mode=1)
+    np.testing.assert_array_equal(scores, want)
