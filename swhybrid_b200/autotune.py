@@ -55,10 +55,18 @@ def reps_for(L: int, reps: int) -> int:
 
 
 def sweep(ctx: capi.Context, lengths, shapes=None, reps: int = 2, log=print,
-          cutovers=(1024, 2048, 4096, 8192, 16384)):
+          cutovers=(1024, 2048, 4096, 8192, 16384), warmup_s: float = 5.0):
     import torch
     shapes = shapes or [(T, R) for T in GROUP_WIDTHS for R in ROWS]
     results = {}
+    # Bring the GPU to its working clock before the first timing: a sweep that
+    # started cold measured its first (shortest) lengths up to 30 % low.
+    warm = torch.from_numpy(synth.query(8999, 2000)).cuda()
+    ctx.set_kernel_config(None)
+    t_end = time.time() + warmup_s
+    while time.time() < t_end:
+        ctx.search_device(warm.data_ptr(), 2000)
+        ctx.sync()
     for L in lengths:
         q = synth.query(9000 + int(L), int(L))
         dq = torch.from_numpy(q).cuda()
