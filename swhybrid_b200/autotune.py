@@ -49,8 +49,8 @@ def reps_for(L: int, reps: int) -> int:
     """Searches timed per shape at query length L: at least `reps`, and
     enough that short queries (a few milliseconds per search on the full DB)
     are timed over about as many cells as a 4,000-residue one.  With one
-    search per shape a sweep picked shapes 7..22 % slower than the committed
-    table's for the queries of 144..310 residues."""
+    search per shape, two sweeps on the same DB picked shapes up to 22 %
+    apart in speed for the queries of 144..310 residues."""
     return max(reps, -(-4000 // max(int(L), 1)))
 
 
