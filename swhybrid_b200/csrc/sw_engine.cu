@@ -742,31 +742,64 @@ const LongKernel* choose_long(sw_ctx* ctx, const sw_kernel_config& cfg, int qlen
     return nullptr;
 }
 
-// sw_get_plan: the bulk range and row segments enqueue_search would run (its
-// cut-over rule: the long-pair kernel takes the pairs above the cut-over when
-// some, but not all, pairs are, and a pipelined shape fits the length; else
-// one shape, the long one without a cut-over, takes every pair).
+// How a plain search of qlen divides the DB's pairs.  With a cut-over (the
+// configured one, else auto_cutover's), the long-pair kernel takes the pairs
+// above it, [0, n_long), when some but not all pairs are, and a pipelined
+// shape fits the length; the bulk launches take the rest with the short shape.
+// Otherwise one shape takes every pair: the long one when no pair is above
+// the cut-over or all are, the short one when no pipelined shape fits.
+struct SearchLayout {
+    sw_kernel_config cfg;
+    int cutover = 0;
+    bool split = false;
+    int64_t n_long = 0;                // pairs of the long-pair kernel (split only)
+    const LongKernel* lk = nullptr;
+    int lpasses = 0, lpipes = 0;
+    size_t lsmem = 0;
+    int bulk_T = 0, bulk_R = 0;        // the bulk launches' shape ...
+    int64_t bulk_b = 0, bulk_e = 0;    // ... pairs ...
+    int bulk_counter = 0;              // ... and claim counter
+};
+
+void layout_search(sw_ctx* ctx, int qlen, SearchLayout* L) {
+    const sw_kernel_config& cfg = L->cfg = choose_config(ctx, qlen);
+    L->cutover = cfg.cutover > 0 ? cfg.cutover : auto_cutover(ctx, cfg, qlen);
+    int64_t n_long = ctx->n_pairs;
+    if (L->cutover > 0) {
+        n_long = 0;
+        while (n_long < ctx->n_pairs && (int)ctx->pair_ncols[n_long] > L->cutover) ++n_long;
+    }
+    L->split = L->cutover > 0 && n_long > 0 && n_long < ctx->n_pairs;
+    if (L->split) {
+        L->lk = choose_long(ctx, cfg, qlen, &L->lpasses, &L->lpipes, &L->lsmem);
+        if (!L->lk) L->split = false;      // no pipelined shape for this length
+    }
+    if (L->split || (n_long < ctx->n_pairs && L->cutover > 0)) {
+        // the short shape: beside the long-pair kernel, or alone for every
+        // pair when no pair is above the cut-over or no pipelined shape fits
+        L->bulk_T = cfg.short_group_width;
+        L->bulk_R = cfg.short_rows_per_thread;
+        L->bulk_b = L->split ? n_long : 0;
+        L->bulk_counter = 1;
+    } else {
+        L->bulk_T = cfg.long_group_width;
+        L->bulk_R = cfg.long_rows_per_thread;
+        L->bulk_b = 0;
+        L->bulk_counter = 0;
+    }
+    L->bulk_e = ctx->n_pairs;
+    L->n_long = L->split ? n_long : 0;
+}
+
+// sw_get_plan: the row segments enqueue_search would run.
 sw_status describe_plan(sw_ctx* ctx, int qlen, sw_plan_step* steps, uint32_t capacity,
                         uint32_t* n_steps) {
-    const sw_kernel_config cfg = choose_config(ctx, qlen);
-    const int cutover = cfg.cutover > 0 ? cfg.cutover : auto_cutover(ctx, cfg, qlen);
-    int64_t n_long = ctx->n_pairs, bulk_b = 0;
-    if (cutover > 0) {
-        n_long = 0;
-        while (n_long < ctx->n_pairs && (int)ctx->pair_ncols[n_long] > cutover) ++n_long;
-    }
-    int T = cfg.long_group_width, R = cfg.long_rows_per_thread;
-    if (n_long < ctx->n_pairs) {
-        T = cfg.short_group_width;
-        R = cfg.short_rows_per_thread;
-        int lp = 0, lg = 0;
-        size_t ls = 0;
-        if (n_long > 0 && choose_long(ctx, cfg, qlen, &lp, &lg, &ls)) bulk_b = n_long;
-    }
-    const WfKernel* k = find_kernel(T, R);
-    if (!k) SW_SET(ctx, SW_ERR_INVALID, "no kernel %dx%d", T, R);
+    SearchLayout L;
+    layout_search(ctx, qlen, &L);
+    const WfKernel* k = find_kernel(L.bulk_T, L.bulk_R);
+    if (!k) SW_SET(ctx, SW_ERR_INVALID, "no kernel %dx%d", L.bulk_T, L.bulk_R);
     RowSeg plan[kMaxRowSegs];
-    const int n = build_plan(ctx, qlen, k, bulk_b, plan);
+    const int n = build_plan(ctx, qlen, k, L.bulk_b, plan);
     *n_steps = (uint32_t)n;
     for (int i = 0; i < n && (uint32_t)i < capacity; ++i) {
         const int rp = plan[i].k->T * plan[i].k->R;
@@ -778,59 +811,39 @@ sw_status describe_plan(sw_ctx* ctx, int qlen, sw_plan_step* steps, uint32_t cap
 sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t* d_scores_rec,
                          unsigned long long** keys_final, uint32_t* launches) {
     cudaStream_t st = ctx->stream;
-    const sw_kernel_config cfg = choose_config(ctx, qlen);
-    ctx->stats.used = cfg;
+    SearchLayout L;
+    layout_search(ctx, qlen, &L);
+    ctx->stats.used = L.cfg;
+    ctx->stats.used.cutover = L.cutover;
     *launches = 0;
-    // pairs [0, n_long) are longer than the cut-over
-    int64_t n_long = ctx->n_pairs;
-    const int cutover = cfg.cutover > 0 ? cfg.cutover : auto_cutover(ctx, cfg, qlen);
-    ctx->stats.used.cutover = cutover;
-    if (cutover > 0) {
-        n_long = 0;
-        while (n_long < ctx->n_pairs && (int)ctx->pair_ncols[n_long] > cutover) ++n_long;
+    const bool split = L.split;
+    const int64_t n_long = L.n_long;
+    const LongKernel* lk = L.lk;
+    const int lpasses = L.lpasses;
+    int lpipes = L.lpipes;
+    if (split) {
+        ctx->stats.used.long_group_width = 32;
+        ctx->stats.used.long_rows_per_thread = lk->R;
     }
-    struct Seg {
-        int T, R;
-        int64_t b, e;
-        int counter;
-    } segs[2] = {{cfg.long_group_width, cfg.long_rows_per_thread, 0, n_long, 0},
-                 {cfg.short_group_width, cfg.short_rows_per_thread, n_long, ctx->n_pairs, 1}};
     const int ovf_thresh = 32767 - std::max(ctx->max_score, 1) + 1;
     // With a cut-over, the long pairs run concurrently on the side stream in
     // sw_long blocks (one warp per query pass, the passes of a pair pipelined
     // across warps, several pipelines per block, one block per SM) on SMs the
     // bulk grid leaves free, as many SMs as the long pairs' share of the
-    // columns.
-    bool split = cutover > 0 && n_long > 0 && n_long < ctx->n_pairs;
-    const LongKernel* lk = nullptr;
-    int lpasses = 0, lpipes = 0;
-    size_t lsmem = 0;
-    if (split) {
-        lk = choose_long(ctx, cfg, qlen, &lpasses, &lpipes, &lsmem);
-        if (!lk) {          // no pipelined shape for this length: one launch for all
-            split = false;
-            segs[0].e = 0;
-            segs[1].b = 0;
-        } else {
-            ctx->stats.used.long_group_width = 32;
-            ctx->stats.used.long_rows_per_thread = lk->R;
-        }
-    }
-    // the bulk launches: the pairs the long-pair kernel does not take, in
-    // the row segments of the length's plan
-    const Seg& bulk = split ? segs[1] : (segs[0].e > segs[0].b ? segs[0] : segs[1]);
+    // columns.  The bulk launches take the other pairs in the row segments of
+    // the length's plan.
     RowSeg plan[kMaxRowSegs];
     int nplan = 0;
     // every shape is checked before anything is launched: a search refused
     // half-way would leave a launch in flight that writes into the next one
-    if (bulk.e > bulk.b) {
-        const WfKernel* k = find_kernel(bulk.T, bulk.R);
-        if (!k) SW_SET(ctx, SW_ERR_INVALID, "no kernel %dx%d", bulk.T, bulk.R);
+    if (L.bulk_e > L.bulk_b) {
+        const WfKernel* k = find_kernel(L.bulk_T, L.bulk_R);
+        if (!k) SW_SET(ctx, SW_ERR_INVALID, "no kernel %dx%d", L.bulk_T, L.bulk_R);
         if (launch_rows(ctx, *k, qlen) == 0)
             SW_SET(ctx, SW_ERR_UNSUPPORTED,
                    "one pass of shape %dx%d does not fit shared memory (profile %zu bytes)",
-                   bulk.T, bulk.R, k->smem(bulk.T * bulk.R));
-        nplan = build_plan(ctx, qlen, k, bulk.b, plan);
+                   L.bulk_T, L.bulk_R, k->smem(L.bulk_T * L.bulk_R));
+        nplan = build_plan(ctx, qlen, k, L.bulk_b, plan);
         if (nplan > 1) {
             ctx->stats.used.short_group_width = plan[0].k->T;
             ctx->stats.used.short_rows_per_thread = plan[0].k->R;
@@ -871,7 +884,7 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
         la.pairs = ctx->d_pairs;
         la.pair_begin = 0;
         la.pair_count = (int)n_long;
-        la.counter = ctx->d_counters + segs[0].counter;
+        la.counter = ctx->d_counters;      // counter 0: the long pairs' claims
         la.query = d_query;
         la.qlen = qlen;
         la.passes = lpasses;
@@ -889,7 +902,7 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
         void* args[] = {&la};
         SW_CUDA(ctx, cudaEventRecord(mk.e[4], ctx->side_stream));
         SW_CUDA(ctx, cudaLaunchKernel(lk->fn, dim3((unsigned)reserved_sms),
-                                      dim3(lpasses * lpipes * 32), args, lsmem, ctx->side_stream));
+                                      dim3(lpasses * lpipes * 32), args, L.lsmem, ctx->side_stream));
         SW_CUDA(ctx, cudaEventRecord(mk.e[5], ctx->side_stream));
         ++*launches;
         ++mk.fp_launches;
@@ -910,12 +923,12 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
             const int rows = std::min(seg_rows, plan[pi].rows - s0);
             const int occ = shape_occupancy(ctx, *k, rows);
             if (r0 > 0)   // the previous launch has claimed every pair
-                SW_CUDA(ctx, cudaMemsetAsync(ctx->d_counters + bulk.counter, 0, sizeof(int), st));
+                SW_CUDA(ctx, cudaMemsetAsync(ctx->d_counters + L.bulk_counter, 0, sizeof(int), st));
             WfArgs a;
             a.db = ctx->d_db;
             a.pairs = ctx->d_pairs;
-            a.pair_begin = (int)bulk.b;
-            a.pair_count = (int)(bulk.e - bulk.b);
+            a.pair_begin = (int)L.bulk_b;
+            a.pair_count = (int)(L.bulk_e - L.bulk_b);
             a.query = d_query + r0;
             a.qlen = rows;
             a.pass0 = passes_before;
@@ -925,7 +938,7 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
             a.bias2 |= a.bias2 << 16;
             a.neg_e = (uint32_t)(uint16_t)(int16_t)(-ctx->params.gap_extend);
             a.neg_e |= a.neg_e << 16;
-            a.counter = ctx->d_counters + bulk.counter;
+            a.counter = ctx->d_counters + L.bulk_counter;
             a.bnd = ctx->d_bnd;
             a.scores = ctx->d_scores;
             a.n_records = (int)ctx->n_records;
@@ -935,7 +948,7 @@ sw_status enqueue_search(sw_ctx* ctx, const uint8_t* d_query, int qlen, int32_t*
             void* args[] = {&a};
             int64_t grid = (int64_t)occ * (ctx->num_sms - reserved_sms);
             const int64_t groups_per_block = k->block / k->T;
-            grid = std::min<int64_t>(grid, ((bulk.e - bulk.b) + groups_per_block - 1) / groups_per_block);
+            grid = std::min<int64_t>(grid, ((L.bulk_e - L.bulk_b) + groups_per_block - 1) / groups_per_block);
             grid = std::max<int64_t>(grid, 1);
             SW_CUDA(ctx, cudaLaunchKernel(k->fn, dim3((unsigned)grid), dim3(k->block), args,
                                           k->smem(rows), st));
