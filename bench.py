@@ -907,8 +907,12 @@ def main(argv=None):
         import datetime
         import torch
         import torch.distributed as dist
-        torch.cuda.set_device(local_rank)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        # NCCL on GPUs; gloo only where there is no GPU (the CPU test of this
+        # control flow, with run_ours stood in for)
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local_rank)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
     if args.shard:
         if world == 1:
             import torch.distributed as dist
@@ -921,10 +925,10 @@ def main(argv=None):
         dist.barrier()
         dist.destroy_process_group()
         return 0
+    # every rank takes the same collective steps: only rank 0 has a line, and
+    # all ranks meet at the final barrier (with or without one)
     line, db, queries, gpu_scores = run_ours(args, rank, world, local_rank)
-    if line is None:
-        return 0
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+    if line is not None and rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb, _, parity = cpu_baseline(db, queries, args.cpu_seconds, gpu_scores)
         if parity is not None:
             line["parity"] = parity

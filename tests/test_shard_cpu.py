@@ -6,6 +6,7 @@ import os
 import socket
 
 import numpy as np
+import torch
 import torch.distributed as dist
 import torch.multiprocessing as mp
 
@@ -162,3 +163,40 @@ def test_bench_shard_mode_two_ranks_equals_whole_db():
     assert got[1][0] is None
     assert line["scaling"] == "strong" and line["n_gpus"] == 2 and line["value"] > 0
     assert line["config"]["rank0_records"][0] == 0
+
+
+def bench_main_worker(rank, world, port, out):
+    """One rank of bench.py's default (weak-scaling) mode, with run_ours
+    stood in for by one max-over-ranks reduction: only rank 0 returns a line."""
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank),
+                      WORLD_SIZE=str(world), LOCAL_RANK=str(rank))
+    import bench
+
+    def fake_run_ours(args, rank, world, local_rank):
+        t = torch.tensor([float(rank)])
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return ({"value": float(t.item())} if rank == 0 else None), None, None, None
+
+    bench.run_ours = fake_run_ours
+    out[rank] = bench.main(["--no-cpu-baseline"])
+
+
+def test_bench_ranks_meet_at_the_end():
+    """Every rank of a multi-GPU bench run takes the same collective steps:
+    the ranks without a line still join rank 0's final barrier, so no rank
+    waits on a peer that has exited (gloo on CPU, two ranks)."""
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as m:
+        out = m.dict()
+        port = free_port()
+        procs = [ctx.Process(target=bench_main_worker, args=(r, 2, port, out)) for r in range(2)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(120)
+        hung = [p.is_alive() for p in procs]
+        for p in procs:
+            if p.is_alive():
+                p.kill()
+        assert not any(hung)
+        assert dict(out) == {0: 0, 1: 0}
