@@ -151,3 +151,34 @@ def test_tuning_table_row_segment_plans():
             assert all(lib_blocks[(T, R)] // T <= 16 for T, R, _ in plan)
         prev = hi
     assert n_plans > 0
+
+
+def test_ctypes_structs_match_the_c_header(tmp_path):
+    """The ctypes mirrors in capi.py have the sizes and field offsets the C
+    compiler gives the structs of include/swb200.h (gcc on a generated
+    program), so the Python binding passes what the library reads."""
+    import subprocess
+    structs = [getattr(capi, n) for n in dir(capi)
+               if n.startswith("sw_") and isinstance(getattr(capi, n), type)
+               and issubclass(getattr(capi, n), ctypes.Structure)]
+    assert len(structs) >= 10
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "swb200.h"', "int main(void) {"]
+    for s in structs:
+        lines.append(f'printf("{s.__name__} size %zu\\n", sizeof({s.__name__}));')
+        for f in s._fields_:
+            lines.append(f'printf("{s.__name__} {f[0]} %zu\\n", offsetof({s.__name__}, {f[0]}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    inc = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "include")
+    subprocess.run(["gcc", "-std=c11", "-I", inc, str(src), "-o", str(exe)], check=True)
+    got = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True,
+                               text=True).stdout.splitlines():
+        name, field, value = line.split()
+        got[(name, field)] = int(value)
+    for s in structs:
+        assert got[(s.__name__, "size")] == ctypes.sizeof(s), s.__name__
+        for f in s._fields_:
+            assert got[(s.__name__, f[0])] == getattr(s, f[0]).offset, (s.__name__, f[0])
