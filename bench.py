@@ -678,9 +678,9 @@ def run_ours(args, rank, world, local_rank):
                        "tuning_table": "swhybrid_b200/tuned/b200.json" if tuned else "cost model",
                        "kernel_config_q144": list(ctx.kernel_config(144)),
                        "kernel_config_q5478": list(ctx.kernel_config(5478)),
-                       "row_segment_plans": {str(int(L)): [list(st) for st in ctx.plan(int(L))]
-                                             for L in sorted({len(q) for q in queries})
-                                             if len(ctx.plan(int(L))) > 1},
+                       "row_segment_plans": {str(L): [list(st) for st in p] for L, p in
+                                             ((L, ctx.plan(L)) for L in sorted({len(q) for q in queries}))
+                                             if len(p) > 1},
                        "db_generate_s": round(gen_s, 2), "db_load_s": round(load_s, 2)},
             "gpu_launches": int(tot.launches),
             "clocks": clocks,
